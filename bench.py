@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""Benchmark of the SPH cutting step (leap_frog::step of iwf_mfree_gpu_3d) on B200.
+
+Workload (one "step" = one full time step of one scene): orthogonal cutting of
+a steel block, 200 x 100 x 50 = 1,000,000 particles, CSPM correction,
+artificial stress and PSE conduction on, Johnson-Cook plasticity, rigid-wedge
+contact, FP32 (the configuration the headline metric is quoted on).  Data is
+synthetic: a seeded jittered lattice and a generated wedge mesh (the reference
+ships no dataset).  The particle state (~0.5 GB) is larger than the 126 MB L2,
+so no L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one process per GPU) every rank steps its own
+independent scene (the reference is single-GPU; scenes shard with no
+collective): weak scaling, value = all ranks' particle-steps / max rank time.
+
+--impl reference times the reference's CPU algorithm -- the FP64 oracle
+restatement, OpenMP on every host core -- on the same scene (a bounded
+sub-block of it per step when the full scene would not finish in minutes).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# ---- algorithmic FLOPs of the pair kernel (counted from the reference's pair
+# formulas, interactions_gpu.cu:152-471 and kernels.cuh:26-92; add/mul = 1,
+# FMA = 2, div/sqrt/exp = 1; the artificial-viscosity branch counted for half
+# of the pairs) ----
+F_CANDIDATE = 8            # distance test of every stencil candidate
+F_CANDIDATE_PSE = 6        # PSE term of every stencil candidate
+F_PAIR = 16 + 24 + 15 + 30 + 15 + 7    # spline, grad v, art. stress, stress divergence, AV, XSPH
+F_PAIR_CSPM = 44 + 15      # CSPM matrix term (with its spline) + corrected gradient
+F_PAIR_BROOKSHAW = 10
+F_PARTICLE_EPILOGUE = 150  # Jaumann, continuity, momentum, corrector, yield check
+
+CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["1m", "8k"], default="1m")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lpp", type=int, default=0, help="lanes per particle (0 = default)")
+    return ap.parse_args()
+
+
+def make_scene(workload: str, seed: int = 0, precision: int = 0):
+    from iwf_mfree_gpu_3d_b200 import scenes
+    if workload == "8k":
+        return scenes.small_scene(seed=seed, precision=precision)
+    return scenes.million_scene(seed=seed, precision=precision)
+
+
+def workload_config(workload: str, sc) -> dict:
+    return {"workload": ("orthogonal cutting 200x100x50 steel block (1,000,000 particles), CSPM + artificial "
+                         "stress + PSE, Johnson-Cook, wedge contact" if workload == "1m" else
+                         "orthogonal cutting 40x20x10 steel block (8,000 particles), Brookshaw, artificial "
+                         "stress, Johnson-Cook, wedge contact"),
+            "particles": sc.n, "dx_cm": 1e-3, "h_over_dx": 1.3, "dt_us": sc.dt,
+            "cspm": bool(sc.options["cspm"]), "conduction": ["none", "brookshaw", "pse"][sc.options["conduction"]],
+            "l2": "inputs larger than L2 (particle state ~0.5 GB)" if workload == "1m" else
+                  "inputs smaller than L2 (8k particles)",
+            "parallelism": "one independent scene per GPU"}
+
+
+# ------------------------------------------------------------ clocks ----
+class ClockSampler:
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={CLOCK_QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------- algorithmic counts ----
+def stencil_counts(sim) -> tuple[float, float]:
+    """(candidates, in-support pairs) summed over the active particles of the
+    last step: candidates from the cell ranges of each particle's 5x5x5
+    stencil, pairs from the kernel's own neighbour counts."""
+    (nx, ny, nz), _, _ = sim.grid()
+    cs, ce = sim.cells()
+    n_act, _ = sim.counts()
+    cnt = np.where(cs >= 0, ce - cs, 0).astype(np.int64)
+    first = np.concatenate([[0], np.cumsum(cnt)])
+    key = sim.get("HASH")[:n_act].astype(np.int64)
+    gi = key // (ny * nz)
+    gj = (key - gi * ny * nz) // nz
+    gk = key % nz
+    z0 = np.maximum(gk - 2, 0)
+    z1 = np.minimum(gk + 2, nz - 1)
+    cand = np.zeros(n_act, np.int64)
+    for dxi in range(-2, 3):
+        for dyi in range(-2, 3):
+            cx, cy = gi + dxi, gj + dyi
+            ok = (cx >= 0) & (cx < nx) & (cy >= 0) & (cy < ny)
+            cb = (np.clip(cx, 0, nx - 1) * ny + np.clip(cy, 0, ny - 1)) * nz
+            cand += np.where(ok, first[cb + z1 + 1] - first[cb + z0], 0)
+    pairs = sim.get("NUM_NBH")[:n_act].astype(np.int64)
+    return float(cand.sum()), float(pairs.sum())
+
+
+def interact_flops(sc, cand: float, pairs: float, n_act: int) -> float:
+    fp = F_PAIR + (F_PAIR_CSPM if sc.options["cspm"] else 0) + (
+        F_PAIR_BROOKSHAW if sc.options["conduction"] == 1 else 0)
+    fc = F_CANDIDATE + (F_CANDIDATE_PSE if sc.options["conduction"] == 2 else 0)
+    return cand * fc + pairs * fp + n_act * F_PARTICLE_EPILOGUE
+
+
+def read_traffic() -> float | None:
+    """DRAM bytes per launch of the pair kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("interact_dram_bytes_per_launch_1m:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# -------------------------------------------------------------- oracle ----
+def cpu_baseline(workload: str, budget_s: float = 20.0) -> dict:
+    """FP64 oracle (OpenMP, every host core) on a bounded sample of the workload."""
+    import oracle
+    oracle.build()
+    cores = os.cpu_count() or 1
+    sc = make_scene(workload)
+    orc = oracle.Oracle(sc, prec=64, threads=cores)
+    t0 = time.perf_counter()
+    orc.step()  # warm-up step
+    t_one = time.perf_counter() - t0
+    nsteps = max(1, min(5, int(budget_s / max(t_one, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        orc.step()
+    t = time.perf_counter() - t0
+    return {"value": sc.n * nsteps / t, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+            "sample": f"{nsteps} FP64 oracle step(s) of the full {sc.n}-particle scene after 1 warm-up step"}
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    import oracle
+    oracle.build()
+    cores = os.cpu_count() or 1
+    sc = make_scene(args.workload)
+    orc = oracle.Oracle(sc, prec=64, threads=cores)
+    t0 = time.perf_counter()
+    orc.step()
+    t_full = time.perf_counter() - t0
+    budget = 150.0
+    total = args.steps + args.warmup
+    if t_full * total <= budget:
+        sample, n_sample = orc, sc.n
+        desc = f"full {sc.n}-particle scene per step"
+    else:
+        # a sub-block of the same lattice (same z depth) sized to the budget
+        from iwf_mfree_gpu_3d_b200 import scenes
+        frac = budget / (t_full * total)
+        nx = max(8, int(200 * math.sqrt(frac)))
+        ny = max(4, int(100 * math.sqrt(frac)))
+        sub = scenes.orthogonal_cutting(nx, ny, 50, cspm=True, conduction=2)
+        sample, n_sample = oracle.Oracle(sub, prec=64, threads=cores), sub.n
+        desc = f"{nx}x{ny}x50 sub-block ({sub.n} particles) of the same scene per step"
+    for _ in range(args.warmup):
+        sample.step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sample.step()
+    t = time.perf_counter() - t0
+    v = n_sample * args.steps / t
+    line = {"metric": "particle-steps/s", "value": v, "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference", "config": workload_config(args.workload, sc),
+            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+                             "sample": "FP64 oracle restatement of leap_frog::step, " + desc},
+            "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- ours ----
+def run_ours(args, rank: int, world: int, local_rank: int, dist):
+    from iwf_mfree_gpu_3d_b200 import api
+    api.set_device(local_rank)
+    sc = make_scene(args.workload, seed=rank)
+    opts = {"lanes_per_particle": args.lpp} if args.lpp else {}
+
+    # --- algorithmic counts of one step (outside the timed region)
+    probe = api.Simulation.from_scene(sc, diagnostics=1, **opts)
+    probe.step()
+    cand, pairs = stencil_counts(probe)
+    n_act = probe.counts()[0]
+    flops_launch = interact_flops(sc, cand, pairs, n_act)
+    probe.close()
+    peak_fp32 = api.fp32_peak_tflops()
+
+    # --- device-resident throughput
+    sim = api.Simulation.from_scene(sc, **opts)
+    for _ in range(max(args.warmup, 3)):
+        sim.step()
+    sim.sync()
+    sim.set_kernel_timing(True)
+    sim.kernel_times()  # reset
+    if dist:
+        dist.barrier()
+    with ClockSampler(local_rank) as clk:
+        sim.sync()
+        sim.timer_start()
+        for _ in range(args.steps):
+            sim.step()
+        ms = sim.timer_stop()
+    ktimes = sim.kernel_times()
+    counters = sim.counters()
+    sim.close()
+    if dist:
+        import torch
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+
+    # --- end to end through the C ABI with host buffers
+    e2e = run_e2e(sc, args, opts, dist, local_rank)
+
+    if rank != 0:
+        return
+    value = sc.n * args.steps * world / (ms * 1e-3)
+    ik_ms, ik_n = ktimes["interact"]
+    ik_avg = ik_ms / max(ik_n, 1)
+    achieved = flops_launch / (ik_avg * 1e-3) / 1e12
+    traffic = read_traffic()
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
+                "frac": achieved / peak_fp32,
+                "traffic": traffic,
+                "kernel": "k_interact (pair loop + fused per-particle rest of the step)",
+                "peak_source": "measured: FP32 FMA-throughput probe on this GPU (mfree_probe_fp32_peak); "
+                               "MEASURED_PEAKS.json holds HBM and bf16 tensor peaks only",
+                "algorithmic_flops_per_launch": flops_launch,
+                "candidates_per_particle": cand / n_act, "pairs_per_particle": pairs / n_act}
+    step_ms_dev = {k: (v[0] / max(v[1], 1)) for k, v in ktimes.items()}
+    line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded jittered lattice, generated wedge tool)",
+            "config": workload_config(args.workload, sc),
+            "roofline": roofline,
+            "e2e": e2e,
+            "gpu_launches": int(sum(v[1] for v in ktimes.values())),
+            "kernel_ms_per_step": step_ms_dev,
+            "clocks": clk.summary(),
+            "counters": counters}
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.workload)
+    print(json.dumps(line), flush=True)
+
+
+def run_e2e(sc, args, opts, dist, local_rank) -> dict:
+    """The same metric through the C ABI from pinned host buffers: the particle
+    arrays are uploaded (mfree_create, as the reference's particle_gpu
+    constructor), every step records and reads back the tool force (as the
+    reference's driver does on its output steps), and the state the user reads
+    (position, velocity, stress, temperature, plastic strain) is copied back at
+    the end; wall clock around all of it."""
+    from iwf_mfree_gpu_3d_b200 import api
+    import torch
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    host = {k: pin(getattr(sc, k)) for k in ("pos", "vel", "rho", "T", "h", "fixed", "tool_p")}
+    h2d = sum(v.nbytes for v in host.values())
+    # warm the path once (module load, allocator)
+    w = api.Simulation(host["pos"], host["vel"], host["rho"], host["h"], T=host["T"], fixed=host["fixed"],
+                       tool_p=host["tool_p"])
+    w.close()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    s = api.Simulation(host["pos"], host["vel"], host["rho"], host["h"], T=host["T"], fixed=host["fixed"],
+                       tool_p=host["tool_p"])
+    s.set_physics(**sc.phys)
+    s.set_correctors(**sc.corr)
+    if sc.joco:
+        s.set_johnson_cook(**sc.joco)
+    s.set_thermal_workpiece(**sc.trml_wp)
+    s.set_thermal_tool(**sc.trml_tool)
+    o = dict(sc.options)
+    o.update(opts)
+    s.set_options(**o)
+    s.set_grid(sc.grid_bbmin, sc.grid_bbmax, sc.grid_h)
+    s.set_blanking(sc.blank_bbmin, sc.blank_bbmax, sc.blank_vmax)
+    for t in sc.tools:
+        s.add_tool(t.verts, t.tris, t.vel, t.contact_alpha, t.mu, t.algorithm)
+    dt = np.float32(sc.dt)
+    s.set_time(float(dt), float(dt))
+    d2h = 0
+    for _ in range(args.steps):
+        s.step(record_forces=True)
+        f = s.tool_forces()
+        d2h += f.nbytes
+    out = [s.get(n) for n in ("POS", "VEL", "S", "T", "EPS_PL")]
+    d2h += sum(a.nbytes for a in out)
+    t = time.perf_counter() - t0
+    s.close()
+    if dist:
+        import torch as _t
+        tt = _t.tensor([t], dtype=_t.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    world = dist.get_world_size() if dist else 1
+    return {"value": sc.n * args.steps * world / t, "unit": "particle-steps/s",
+            "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
+            "note": "wall clock: context creation from pinned host arrays, setup, steps with a per-step tool-force "
+                    "read-back, final read-back of POS/VEL/S/T/EPS_PL; state bytes amortised over the steps"}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1 and args.impl == "ours":  # the reference arm runs on rank 0 alone
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local_rank, dist)
+    finally:
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,252 @@
+/*
+ * mfree.h -- C ABI of the B200-native SPH cutting step (libmfree.so).
+ *
+ * One call of mfree_step() is one call of leap_frog::step() of iwf_mfree_gpu_3d
+ * (src/leap_frog.cu:121-195): blanking, cell-list hash + stable sort, predictor,
+ * EOS + artificial stress, pair interactions (Gray/Monaghan stress divergence,
+ * artificial viscosity, XSPH, CSPM, Brookshaw or PSE conduction), Jaumann rate,
+ * continuity, momentum, advection, corrector, Johnson-Cook radial return, rigid
+ * tool contact with friction, friction heating, boundary conditions and the
+ * translation of tool particles.
+ *
+ * The reference has no library boundary: its driver links C++ classes and
+ * writes process globals.  Every entry point below names the reference call it
+ * stands in for.  Conventions:
+ *   - every call returns an int status (MFREE_OK = 0, negative on error; the
+ *     message is in mfree_last_error()); nothing calls exit();
+ *   - a context owns its device memory and frees it in mfree_destroy();
+ *   - host buffers are caller-owned and copied;
+ *   - calls on one context are not thread-safe; separate contexts are
+ *     independent (the reference keeps its state in process globals);
+ *   - arrays are in the current (sorted) particle order, as in the reference,
+ *     with the reference's per-field layout (particle_gpu.h:36-99).
+ *
+ * Units are the reference's cm-g-us system (stress in Mbar).
+ */
+#ifndef MFREE_H_
+#define MFREE_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define MFREE_OK              0
+#define MFREE_ERR_ARG        -1  /* bad argument or call order            */
+#define MFREE_ERR_CUDA       -2  /* CUDA runtime error                    */
+#define MFREE_ERR_OOM        -3  /* device allocation failed              */
+#define MFREE_ERR_NUMERIC    -4  /* device-reported numerical failure     */
+#define MFREE_ERR_IO         -5  /* scene file could not be read/parsed   */
+#define MFREE_ERR_EMPTY      -6  /* every particle left the box: the
+                                    reference prints and exit(0)s
+                                    (grid_gpu_base.cu:159-163)            */
+
+/* ---- constant records (constants_structs.h:25-92) ----------------------- */
+typedef struct { float E, nu, rho0, K, G, mass; } mfree_phys;          /* phys_constants */
+typedef struct { float cp, tq, k, alpha, T_init, eta; } mfree_trml;    /* trml_constants */
+typedef struct { float wdeltap, stresseps, xspheps, alpha, beta, eta; } mfree_corr; /* corr_constants */
+typedef struct { float A, B, C, n, m, Tmelt, Tref, eps_dot_ref, clamp_temp; } mfree_joco; /* joco_constants */
+
+/* ---- switches that are #defines in the reference (types.h:32-108) ------- */
+#define MFREE_COND_NONE      0
+#define MFREE_COND_BROOKSHAW 1   /* Thermal_Conduction_Brookshaw (types.h:104) */
+#define MFREE_COND_PSE       2   /* Thermal_Conduction_PSE (types.h:105)       */
+
+typedef struct {
+    int cspm;               /* CSPM kernel correction (types.h:102)                  */
+    int conduction;         /* MFREE_COND_*                                            */
+    int precision;          /* 0: FP32 state; 1: FP32 bulk + compensated hi/lo
+                               position and velocity in predictor/corrector          */
+    int max_secant_iter;    /* Johnson-Cook secant limit (plasticity.cuh:66: 100)     */
+    int lanes_per_particle; /* interaction tiling: 4, 8, 16 or 32 lanes of a warp per
+                               particle; 0 picks the tuned default                   */
+    int diagnostics;        /* 1: keep neighbour counts, half-step positions and
+                               contact normals for mfree_get_field()                  */
+    int friction_tool_vel;  /* 1: subtract the tool velocity in the friction slip
+                               velocity.  The reference never uploads its tool_vel
+                               constant (tool_3d_gpu.cu:26,528), so 0 matches it.    */
+} mfree_options;
+
+/* ---- fields for mfree_get_field / mfree_set_field ------------------------
+ * element layout = the reference's particle_gpu member (float4 = 4 floats,
+ * float3 = 3 floats, mat3x3 = 9 floats in GLM column-major order m[col][row]). */
+enum mfree_field {
+    MFREE_POS = 0,        /* float4 */
+    MFREE_VEL,            /* float4 */
+    MFREE_VEL_BC,         /* float4 */
+    MFREE_H,              /* float  */
+    MFREE_RHO,            /* float  */
+    MFREE_P,              /* float  (pressure of the last half step)           */
+    MFREE_S,              /* mat3x3 */
+    MFREE_R,              /* mat3x3 (artificial stress of the last half step)  */
+    MFREE_FC,             /* float3 */
+    MFREE_FT,             /* float3 */
+    MFREE_NRM,            /* float3 contact normal (diagnostics only)          */
+    MFREE_FIXED,          /* float  */
+    MFREE_BLANKED,        /* float  */
+    MFREE_TOOL_PARTICLE,  /* float  */
+    MFREE_EPS_PL,         /* float  */
+    MFREE_EPS_PL_DOT,     /* float  */
+    MFREE_T,              /* float  */
+    MFREE_POS_T,          /* float3 */
+    MFREE_VEL_T,          /* float3 */
+    MFREE_RHO_T,          /* float  */
+    MFREE_S_T,            /* mat3x3 */
+    MFREE_T_T,            /* float  */
+    MFREE_NUM_NBH,        /* int    (diagnostics only)                         */
+    MFREE_IDX,            /* int    sort permutation of the last step           */
+    MFREE_HASH,           /* int    sorted cell ids, INT_MAX = blanked          */
+    MFREE_ID,             /* int    particle id = index at creation (new)      */
+    MFREE_POS_HALF,       /* float4 half-step positions (diagnostics only)     */
+    MFREE_NUM_FIELDS
+};
+
+/* per-context counters of device-detected conditions */
+typedef struct {
+    int64_t steps;              /* steps taken                                          */
+    int64_t secant_failures;    /* radial returns that hit the iteration limit
+                                   (the reference printf's, actions_gpu.cu:415-418)     */
+    int64_t out_of_grid;        /* non-blanked particles outside the cell grid; they are
+                                   blanked (the reference prints ALARM and writes out of
+                                   bounds, grid_gpu_green.cu:56-58)                     */
+    int64_t contact_search_cap; /* contact shell searches stopped by the bound          */
+    int64_t nan_blanked;        /* particles kept blanked because a rate is NaN/Inf     */
+} mfree_counters;
+
+typedef struct mfree_ctx mfree_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+
+/* particle_gpu(pos, vel, rho, T, h, fixed, tool_p, N) (particle_gpu.h:300-304,
+ * particle_gpu.cu:20-117).  pos/vel: n float4; T, fixed, tool_p may be NULL
+ * (zeros, as the shorter reference constructors).  stream: the cudaStream_t
+ * every call of this context is ordered on, or NULL for a stream the context
+ * creates (and destroys) itself. */
+int mfree_create(int n, const float *pos4, const float *vel4, const float *rho,
+                 const float *T, const float *h, const float *fixed,
+                 const float *tool_p, void *stream, mfree_ctx **out);
+int mfree_destroy(mfree_ctx *ctx);
+const char *mfree_last_error(void);
+
+/* actions_setup_physical_constants + interactions_setup_physical_constants
+ * (actions_gpu.cu:659-665, interactions_gpu.cu:564-569) */
+int mfree_set_physics(mfree_ctx *ctx, const mfree_phys *phys);
+/* actions_/interactions_setup_corrector_constants (actions_gpu.cu:667-674,
+ * interactions_gpu.cu:571-573) */
+int mfree_set_correctors(mfree_ctx *ctx, const mfree_corr *corr);
+/* actions_setup_johnson_cook_constants (actions_gpu.cu:676-679): switches
+ * plasticity on */
+int mfree_set_johnson_cook(mfree_ctx *ctx, const mfree_joco *joco);
+/* actions_setup_thermal_constants_wp + interactions_setup_thermal_constants_workpiece
+ * (actions_gpu.cu:681-698, interactions_gpu.cu:575-590) */
+int mfree_set_thermal_workpiece(mfree_ctx *ctx, const mfree_trml *trml);
+/* actions_setup_thermal_constants_tool + interactions_setup_thermal_constants_tool
+ * (actions_gpu.cu:700-710, interactions_gpu.cu:592-608) */
+int mfree_set_thermal_tool(mfree_ctx *ctx, const mfree_trml *trml);
+int mfree_set_options(mfree_ctx *ctx, const mfree_options *opt);
+int mfree_get_options(const mfree_ctx *ctx, mfree_options *opt);
+
+/* grid_gpu_green(num_part, bbmin, bbmax, h): locked cell grid
+ * (grid_gpu_green.cu:342-346, grid_gpu_base.cu:237-273) */
+int mfree_set_grid(mfree_ctx *ctx, const float bbmin[3], const float bbmax[3], float h);
+/* grid_base::set_bbox_vel (grid_gpu_base.cu:113-115): moving locked grid */
+int mfree_set_grid_velocity(mfree_ctx *ctx, const float vel[3]);
+/* blanking(bbmin, bbmax, [bbvel,] max_vel) (blanking.cpp:29-33) */
+int mfree_set_blanking(mfree_ctx *ctx, const float bbmin[3], const float bbmax[3],
+                       const float *bbvel3, float max_vel);
+
+/* global_time_dt / global_time_current / global_time_step (mfree_gpu_3d.cpp:45-48).
+ * mfree_step() uses t_current and then adds dt to it, as main() does after each
+ * loop iteration (mfree_gpu_3d.cpp:203-204). */
+int mfree_set_time(mfree_ctx *ctx, float dt, float t_current);
+int mfree_get_time(const mfree_ctx *ctx, float *dt, float *t_current);
+
+/* ---- tools --------------------------------------------------------------- */
+#define MFREE_CONTACT_HASHED     0  /* tool_3d_gpu::contact_algorithm::spatial_hashing */
+#define MFREE_CONTACT_EXHAUSTIVE 1  /* tool_3d_gpu::contact_algorithm::exhaustive      */
+
+/* mesh_compute_vertex_normals + mesh_average_edge_length + tool_3d(tris, pos, h)
+ * + tool_3d_gpu(tool, vel, phys, alpha) + set_mu + set_algorithm_type
+ * (surface_tri_mesh.cpp:410-584, tool_3d.cpp:294-360, tool_3d_gpu.cu:688-812).
+ * verts: nv*3 floats; tris: nt*3 vertex indices of a closed manifold.
+ * The contact mass is the particle mass of mfree_set_physics. */
+int mfree_add_tool(mfree_ctx *ctx, const float *verts, int nv, const int *tris, int nt,
+                   const float vel[3], float contact_alpha, float mu, int algorithm,
+                   int *tool_index);
+/* tool_3d_gpu::set_birth_death (tool_3d_gpu.cu:698-701) */
+int mfree_tool_set_birth_death(mfree_ctx *ctx, int tool, float birth, float death);
+/* tool_forces::get_forces_host (tool_3d_gpu.cu:34-38): 3 floats per tool,
+ * summed over the particles in a fixed order (the reference uses atomicAdd) */
+int mfree_get_tool_forces(mfree_ctx *ctx, float *out3);
+/* tool geometry of the setup: boxed-triangle count, tri-grid cells and bbox */
+int mfree_get_tool_info(mfree_ctx *ctx, int tool, int *num_tris, int *num_boxed,
+                        int *grid_n3, float *bbmin3, float *bbmax3, float *cell_dx);
+/* per-triangle normals after setup: face n, vertex np1..3, edge ne1..3 as
+ * 7 float3 per triangle in input order (surface_tri_mesh.h:39-63) */
+int mfree_get_tool_normals(mfree_ctx *ctx, int tool, float *out21);
+/* triangle grid of the setup: cells = CSR offsets (grid cells + 1 entries) into
+ * the boxed triangles, boxed_src = input index of each boxed triangle
+ * (grid_cpu_tri::get_cells, grid_cpu_tri.cpp:96-175) */
+int mfree_get_tool_cells(mfree_ctx *ctx, int tool, int *cells, int *boxed_src);
+
+/* ---- stepping ------------------------------------------------------------ */
+/* leap_frog::step(particles, grid, record_forces) (leap_frog.cu:121-195) */
+int mfree_step(mfree_ctx *ctx, int record_forces);
+/* nsteps calls of mfree_step; forces recorded every record_every steps
+ * (0: never).  With use_graph != 0 the step is captured once into a CUDA graph
+ * and replayed. */
+int mfree_advance(mfree_ctx *ctx, int nsteps, int record_every, int use_graph);
+/* block the host until the context's stream is idle */
+int mfree_sync(mfree_ctx *ctx);
+
+/* ---- state access -------------------------------------------------------- */
+int mfree_get_counts(const mfree_ctx *ctx, int *n_active, int *n_init);
+/* count elements of one particle's entry of a field (4 for float4 ...) */
+int mfree_field_width(int field);
+/* copy a whole field (n_init entries) to / from host memory */
+int mfree_get_field(mfree_ctx *ctx, int field, void *out);
+int mfree_set_field(mfree_ctx *ctx, int field, const void *in);
+/* the same in double: MFREE_POS and MFREE_VEL return hi + lo of the
+ * compensated accumulation when options.precision = 1 */
+int mfree_get_field_f64(mfree_ctx *ctx, int field, double *out);
+/* cell ranges in the reference format (cell_start/cell_end, -1 = empty;
+ * grid_gpu_green.cu:24-70,277-278), num_cell entries each */
+int mfree_get_cells(mfree_ctx *ctx, int *cell_start, int *cell_end);
+/* grid geometry after set_geometry (grid_gpu_base.cu:237-273) */
+int mfree_get_grid(const mfree_ctx *ctx, long *nx, long *ny, long *nz,
+                   float *bbmin3, float *dx);
+int mfree_get_counters(mfree_ctx *ctx, mfree_counters *out);
+
+/* ---- measurement (no reference counterpart) --------------------------------
+ * Per-kernel device time of eager mfree_step calls: when on, CUDA events
+ * bracket every kernel of a step on the context's stream.  Kernel order:
+ * clock, hash, scan_reduce, scan_top, scan_down, scatter, cell_fixup,
+ * gather_predict, interact, finalize, force_final (MFREE_NUM_KERNELS). */
+#define MFREE_NUM_KERNELS 11
+int mfree_set_kernel_timing(mfree_ctx *ctx, int on);
+/* accumulated milliseconds and launch counts per kernel since the last call;
+ * synchronises the stream and resets the accumulators */
+int mfree_get_kernel_times(mfree_ctx *ctx, double *ms, int *launches);
+/* sustained FP32 FMA throughput of the current device in TFLOP/s */
+int mfree_probe_fp32_peak(double *tflops);
+/* device-timed region on the context's stream (CUDA events) */
+int mfree_timer_start(mfree_ctx *ctx);
+int mfree_timer_stop(mfree_ctx *ctx, double *ms);
+/* select the CUDA device for the contexts created afterwards on this thread
+ * (one process per GPU) */
+int mfree_set_device(int device);
+
+/* ---- scene files (the reference's setup readers) ------------------------- */
+/* json_read_triangles (json_reader.cpp:108-117): MeshLab JSON */
+int mfree_read_mesh_json(const char *path, float **verts, int *nv, int **tris, int *nt);
+/* ldynak_read_triangles_from_tetmesh (ldynak_reader.cpp:371-434): LS-DYNA .k */
+int mfree_read_mesh_ldynak(const char *path, float **verts, int *nv, int **tris, int *nt);
+void mfree_free(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MFREE_H_ */

@@ -1,0 +1,416 @@
+"""Python binding of libmfree.so (include/mfree.h) over ctypes.
+
+The reference drives its step from C++ (src/mfree_gpu_3d.cpp:75-218): it builds
+a ``particle_gpu`` from host arrays, uploads the constant records with
+``actions_setup_*`` / ``interactions_setup_*``, creates the locked grid, the
+blanking box and the tools, then calls ``leap_frog::step`` once per time step.
+``Simulation`` mirrors those calls one to one on top of the C ABI; every call
+raises ``MfreeError`` on a non-zero status.  There is no CPU fallback: if the
+CUDA library cannot be loaded, construction fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libmfree.so")
+
+FIELDS = ["POS", "VEL", "VEL_BC", "H", "RHO", "P", "S", "R", "FC", "FT", "NRM", "FIXED", "BLANKED",
+          "TOOL_PARTICLE", "EPS_PL", "EPS_PL_DOT", "T", "POS_T", "VEL_T", "RHO_T", "S_T", "T_T", "NUM_NBH",
+          "IDX", "HASH", "ID", "POS_HALF"]
+FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
+INT_FIELDS = {"NUM_NBH", "IDX", "HASH", "ID"}
+
+COND_NONE, COND_BROOKSHAW, COND_PSE = 0, 1, 2
+CONTACT_HASHED, CONTACT_EXHAUSTIVE = 0, 1
+
+# every symbol include/mfree.h declares
+EXPORTS = [
+    "mfree_create", "mfree_destroy", "mfree_last_error", "mfree_set_physics", "mfree_set_correctors",
+    "mfree_set_johnson_cook", "mfree_set_thermal_workpiece", "mfree_set_thermal_tool", "mfree_set_options",
+    "mfree_get_options", "mfree_set_grid", "mfree_set_grid_velocity", "mfree_set_blanking", "mfree_set_time",
+    "mfree_get_time", "mfree_add_tool", "mfree_tool_set_birth_death", "mfree_get_tool_forces",
+    "mfree_get_tool_info", "mfree_get_tool_normals", "mfree_get_tool_cells", "mfree_step", "mfree_advance",
+    "mfree_sync", "mfree_get_counts", "mfree_field_width", "mfree_get_field", "mfree_set_field",
+    "mfree_get_field_f64", "mfree_get_cells", "mfree_get_grid", "mfree_get_counters", "mfree_read_mesh_json",
+    "mfree_read_mesh_ldynak", "mfree_free", "mfree_set_kernel_timing", "mfree_get_kernel_times",
+    "mfree_probe_fp32_peak", "mfree_timer_start", "mfree_timer_stop", "mfree_set_device",
+]
+KERNELS = ["clock", "hash", "scan_reduce", "scan_top", "scan_down", "scatter", "cell_fixup", "gather_predict",
+           "interact", "finalize", "force_final"]
+
+
+class MfreeError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"mfree status {status}: {msg}")
+        self.status = status
+
+
+class Phys(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("E", "nu", "rho0", "K", "G", "mass")]
+
+
+class Trml(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("cp", "tq", "k", "alpha", "T_init", "eta")]
+
+
+class Corr(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("wdeltap", "stresseps", "xspheps", "alpha", "beta", "eta")]
+
+
+class Joco(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("A", "B", "C", "n", "m", "Tmelt", "Tref", "eps_dot_ref", "clamp_temp")]
+
+
+class Options(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("cspm", "conduction", "precision", "max_secant_iter",
+                                       "lanes_per_particle", "diagnostics", "friction_tool_vel")]
+
+
+class Counters(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("steps", "secant_failures", "out_of_grid", "contact_search_cap",
+                                         "nan_blanked")]
+
+
+_lib = None
+
+
+def lib(path: str = LIB_PATH):
+    """Load libmfree.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with python -m iwf_mfree_gpu_3d_b200.build")
+    L = C.CDLL(path)
+    I, F, P = C.c_int, C.c_float, C.c_void_p
+    fp = C.POINTER(C.c_float)
+    ip = C.POINTER(C.c_int)
+    L.mfree_last_error.restype = C.c_char_p
+    L.mfree_create.argtypes = [I, fp, fp, fp, fp, fp, fp, fp, P, C.POINTER(P)]
+    L.mfree_destroy.argtypes = [P]
+    L.mfree_set_physics.argtypes = [P, C.POINTER(Phys)]
+    L.mfree_set_correctors.argtypes = [P, C.POINTER(Corr)]
+    L.mfree_set_johnson_cook.argtypes = [P, C.POINTER(Joco)]
+    L.mfree_set_thermal_workpiece.argtypes = [P, C.POINTER(Trml)]
+    L.mfree_set_thermal_tool.argtypes = [P, C.POINTER(Trml)]
+    L.mfree_set_options.argtypes = [P, C.POINTER(Options)]
+    L.mfree_get_options.argtypes = [P, C.POINTER(Options)]
+    L.mfree_set_grid.argtypes = [P, fp, fp, F]
+    L.mfree_set_grid_velocity.argtypes = [P, fp]
+    L.mfree_set_blanking.argtypes = [P, fp, fp, fp, F]
+    L.mfree_set_time.argtypes = [P, F, F]
+    L.mfree_get_time.argtypes = [P, fp, fp]
+    L.mfree_add_tool.argtypes = [P, fp, I, ip, I, fp, F, F, I, ip]
+    L.mfree_tool_set_birth_death.argtypes = [P, I, F, F]
+    L.mfree_get_tool_forces.argtypes = [P, fp]
+    L.mfree_get_tool_info.argtypes = [P, I, ip, ip, ip, fp, fp, fp]
+    L.mfree_get_tool_normals.argtypes = [P, I, fp]
+    L.mfree_get_tool_cells.argtypes = [P, I, ip, ip]
+    L.mfree_step.argtypes = [P, I]
+    L.mfree_advance.argtypes = [P, I, I, I]
+    L.mfree_sync.argtypes = [P]
+    L.mfree_get_counts.argtypes = [P, ip, ip]
+    L.mfree_field_width.argtypes = [I]
+    L.mfree_get_field.argtypes = [P, I, P]
+    L.mfree_set_field.argtypes = [P, I, P]
+    L.mfree_get_field_f64.argtypes = [P, I, C.POINTER(C.c_double)]
+    L.mfree_get_cells.argtypes = [P, ip, ip]
+    L.mfree_get_grid.argtypes = [P, C.POINTER(C.c_long), C.POINTER(C.c_long), C.POINTER(C.c_long), fp, fp]
+    L.mfree_get_counters.argtypes = [P, C.POINTER(Counters)]
+    L.mfree_read_mesh_json.argtypes = [C.c_char_p, C.POINTER(fp), ip, C.POINTER(ip), ip]
+    L.mfree_read_mesh_ldynak.argtypes = [C.c_char_p, C.POINTER(fp), ip, C.POINTER(ip), ip]
+    L.mfree_free.argtypes = [P]
+    L.mfree_set_kernel_timing.argtypes = [P, I]
+    L.mfree_get_kernel_times.argtypes = [P, C.POINTER(C.c_double), ip]
+    L.mfree_probe_fp32_peak.argtypes = [C.POINTER(C.c_double)]
+    L.mfree_timer_start.argtypes = [P]
+    L.mfree_timer_stop.argtypes = [P, C.POINTER(C.c_double)]
+    L.mfree_set_device.argtypes = [I]
+    _lib = L
+    return L
+
+
+def _check(st: int):
+    if st != 0:
+        raise MfreeError(st, lib().mfree_last_error().decode())
+
+
+def _f32(a):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a, a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _mk(cls, d):
+    return cls(**{k: d[k] for k, _ in cls._fields_})
+
+
+def set_device(device: int):
+    """Select the CUDA device of the contexts created afterwards (one process per GPU)."""
+    _check(lib().mfree_set_device(int(device)))
+
+
+def fp32_peak_tflops() -> float:
+    """Measured sustained FP32 FMA throughput of the current device (TFLOP/s)."""
+    v = C.c_double()
+    _check(lib().mfree_probe_fp32_peak(C.byref(v)))
+    return v.value
+
+
+def read_mesh(path: str):
+    """Read a MeshLab .json or LS-DYNA .k tool mesh: (verts (nv,3) float32, tris (nt,3) int32)."""
+    L = lib()
+    vp = C.POINTER(C.c_float)()
+    tp = C.POINTER(C.c_int)()
+    nv = C.c_int()
+    nt = C.c_int()
+    fn = L.mfree_read_mesh_json if path.endswith(".json") else L.mfree_read_mesh_ldynak
+    st = fn(path.encode(), C.byref(vp), C.byref(nv), C.byref(tp), C.byref(nt))
+    if st != 0:
+        raise MfreeError(st, f"could not read mesh {path}")
+    try:
+        v = np.ctypeslib.as_array(vp, shape=(nv.value * 3,)).copy().reshape(-1, 3)
+        t = np.ctypeslib.as_array(tp, shape=(nt.value * 3,)).copy().reshape(-1, 3)
+    finally:
+        L.mfree_free(vp)
+        L.mfree_free(tp)
+    return v, t
+
+
+class Simulation:
+    """One cutting scene on the GPU: particle_gpu + leap_frog + grid + blanking + tools."""
+
+    def __init__(self, pos4, vel4, rho, h, T=None, fixed=None, tool_p=None, stream: Optional[int] = None):
+        L = lib()
+        self.L = L
+        n = int(np.asarray(pos4).shape[0])
+        keep = []
+
+        def arg(a):
+            if a is None:
+                return None
+            a, p = _f32(a)
+            keep.append(a)
+            return p
+
+        h_ = C.c_void_p()
+        _check(L.mfree_create(n, arg(pos4), arg(vel4), arg(rho), arg(T), arg(h), arg(fixed), arg(tool_p),
+                              C.c_void_p(stream) if stream else None, C.byref(h_)))
+        self.h = h_
+        self.n_init = n
+        self.num_tools = 0
+
+    # -- the reference's setup calls --
+    def set_physics(self, **kw):
+        self._phys = _mk(Phys, kw)
+        _check(self.L.mfree_set_physics(self.h, C.byref(self._phys)))
+
+    def set_correctors(self, **kw):
+        self._corr = _mk(Corr, kw)
+        _check(self.L.mfree_set_correctors(self.h, C.byref(self._corr)))
+
+    def set_johnson_cook(self, **kw):
+        self._joco = _mk(Joco, kw)
+        _check(self.L.mfree_set_johnson_cook(self.h, C.byref(self._joco)))
+
+    def set_thermal_workpiece(self, **kw):
+        self._twp = _mk(Trml, kw)
+        _check(self.L.mfree_set_thermal_workpiece(self.h, C.byref(self._twp)))
+
+    def set_thermal_tool(self, **kw):
+        self._ttool = _mk(Trml, kw)
+        _check(self.L.mfree_set_thermal_tool(self.h, C.byref(self._ttool)))
+
+    def set_options(self, **kw):
+        o = Options(cspm=0, conduction=COND_BROOKSHAW, precision=0, max_secant_iter=100, lanes_per_particle=0,
+                    diagnostics=0, friction_tool_vel=0)
+        for k, v in kw.items():
+            setattr(o, k, int(v))
+        self._opt = o
+        _check(self.L.mfree_set_options(self.h, C.byref(o)))
+
+    def options(self) -> dict:
+        o = Options()
+        _check(self.L.mfree_get_options(self.h, C.byref(o)))
+        return {k: getattr(o, k) for k, _ in Options._fields_}
+
+    def set_grid(self, bbmin, bbmax, h: float):
+        lo, plo = _f32(bbmin)
+        hi, phi = _f32(bbmax)
+        _check(self.L.mfree_set_grid(self.h, plo, phi, float(h)))
+
+    def set_grid_velocity(self, vel):
+        v, p = _f32(vel)
+        _check(self.L.mfree_set_grid_velocity(self.h, p))
+
+    def set_blanking(self, bbmin, bbmax, max_vel: float, bbvel=None):
+        lo, plo = _f32(bbmin)
+        hi, phi = _f32(bbmax)
+        vv = None
+        if bbvel is not None:
+            vv_a, vv = _f32(bbvel)
+        _check(self.L.mfree_set_blanking(self.h, plo, phi, vv, float(max_vel)))
+
+    def set_time(self, dt: float, t: float):
+        _check(self.L.mfree_set_time(self.h, float(dt), float(t)))
+
+    def time(self):
+        dt = C.c_float()
+        t = C.c_float()
+        _check(self.L.mfree_get_time(self.h, C.byref(dt), C.byref(t)))
+        return dt.value, t.value
+
+    def add_tool(self, verts, tris, vel, contact_alpha: float = 0.1, mu: float = 0.0,
+                 algorithm: int = CONTACT_HASHED) -> int:
+        v, pv = _f32(np.asarray(verts).reshape(-1))
+        t = np.ascontiguousarray(np.asarray(tris, np.int32).reshape(-1))
+        ve, pve = _f32(vel)
+        k = C.c_int()
+        _check(self.L.mfree_add_tool(self.h, pv, len(v) // 3, t.ctypes.data_as(C.POINTER(C.c_int)), len(t) // 3,
+                                     pve, float(contact_alpha), float(mu), int(algorithm), C.byref(k)))
+        self.num_tools += 1
+        return k.value
+
+    def tool_info(self, k: int = 0) -> dict:
+        nt, nb = C.c_int(), C.c_int()
+        n3 = (C.c_int * 3)()
+        lo = (C.c_float * 3)()
+        hi = (C.c_float * 3)()
+        dx = C.c_float()
+        _check(self.L.mfree_get_tool_info(self.h, k, C.byref(nt), C.byref(nb), n3, lo, hi, C.byref(dx)))
+        return dict(num_tris=nt.value, num_boxed=nb.value, n3=tuple(n3), bbmin=tuple(lo), bbmax=tuple(hi),
+                    dx=dx.value)
+
+    def tool_normals(self, k: int = 0) -> np.ndarray:
+        nt = self.tool_info(k)["num_tris"]
+        out = np.zeros(nt * 21, np.float32)
+        _check(self.L.mfree_get_tool_normals(self.h, k, out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out.reshape(nt, 7, 3)
+
+    def tool_cells(self, k: int = 0):
+        info = self.tool_info(k)
+        nc = info["n3"][0] * info["n3"][1] * info["n3"][2]
+        cells = np.zeros(nc + 1, np.int32)
+        src = np.zeros(max(1, info["num_boxed"]), np.int32)
+        ip = C.POINTER(C.c_int)
+        _check(self.L.mfree_get_tool_cells(self.h, k, cells.ctypes.data_as(ip), src.ctypes.data_as(ip)))
+        return cells, src[: info["num_boxed"]]
+
+    def tool_forces(self) -> np.ndarray:
+        out = np.zeros(3 * max(1, self.num_tools), np.float32)
+        _check(self.L.mfree_get_tool_forces(self.h, out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out.reshape(-1, 3)[: self.num_tools]
+
+    # -- stepping --
+    def step(self, record_forces: bool = False):
+        _check(self.L.mfree_step(self.h, int(record_forces)))
+
+    def advance(self, nsteps: int, record_every: int = 0, use_graph: bool = True):
+        _check(self.L.mfree_advance(self.h, int(nsteps), int(record_every), int(use_graph)))
+
+    def set_kernel_timing(self, on: bool = True):
+        _check(self.L.mfree_set_kernel_timing(self.h, int(on)))
+
+    def kernel_times(self) -> dict:
+        """{kernel: (total ms, launches)} of the eager steps since the last call."""
+        ms = (C.c_double * len(KERNELS))()
+        n = (C.c_int * len(KERNELS))()
+        _check(self.L.mfree_get_kernel_times(self.h, ms, n))
+        return {k: (ms[i], n[i]) for i, k in enumerate(KERNELS)}
+
+    def timer_start(self):
+        _check(self.L.mfree_timer_start(self.h))
+
+    def timer_stop(self) -> float:
+        """Device milliseconds since timer_start (CUDA events on the context's stream)."""
+        ms = C.c_double()
+        _check(self.L.mfree_timer_stop(self.h, C.byref(ms)))
+        return ms.value
+
+    def sync(self):
+        _check(self.L.mfree_sync(self.h))
+
+    # -- state --
+    def counts(self):
+        n = C.c_int()
+        ni = C.c_int()
+        _check(self.L.mfree_get_counts(self.h, C.byref(n), C.byref(ni)))
+        return n.value, ni.value
+
+    def counters(self) -> dict:
+        c = Counters()
+        _check(self.L.mfree_get_counters(self.h, C.byref(c)))
+        return {k: getattr(c, k) for k, _ in Counters._fields_}
+
+    def get(self, name: str) -> np.ndarray:
+        f = FIELD_ID[name]
+        w = self.L.mfree_field_width(f)
+        dt = np.int32 if name in INT_FIELDS else np.float32
+        out = np.zeros(self.n_init * w, dt)
+        _check(self.L.mfree_get_field(self.h, f, out.ctypes.data_as(C.c_void_p)))
+        return out.reshape(self.n_init, w) if w > 1 else out
+
+    def get64(self, name: str) -> np.ndarray:
+        f = FIELD_ID[name]
+        w = self.L.mfree_field_width(f)
+        out = np.zeros(self.n_init * w, np.float64)
+        _check(self.L.mfree_get_field_f64(self.h, f, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out.reshape(self.n_init, w) if w > 1 else out
+
+    def set(self, name: str, values):
+        a = np.ascontiguousarray(values, dtype=np.float32).reshape(-1)
+        _check(self.L.mfree_set_field(self.h, FIELD_ID[name], a.ctypes.data_as(C.c_void_p)))
+
+    def grid(self):
+        nx, ny, nz = C.c_long(), C.c_long(), C.c_long()
+        lo = (C.c_float * 3)()
+        dx = C.c_float()
+        _check(self.L.mfree_get_grid(self.h, C.byref(nx), C.byref(ny), C.byref(nz), lo, C.byref(dx)))
+        return (nx.value, ny.value, nz.value), tuple(lo), dx.value
+
+    def cells(self):
+        (nx, ny, nz), _, _ = self.grid()
+        cs = np.zeros(nx * ny * nz, np.int32)
+        ce = np.zeros(nx * ny * nz, np.int32)
+        ip = C.POINTER(C.c_int)
+        _check(self.L.mfree_get_cells(self.h, cs.ctypes.data_as(ip), ce.ctypes.data_as(ip)))
+        return cs, ce
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.L.mfree_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- building from a scene description --
+    @classmethod
+    def from_scene(cls, scene, stream: Optional[int] = None, **option_overrides) -> "Simulation":
+        """Set up a scene the way the reference's setup functions do."""
+        s = cls(scene.pos, scene.vel, scene.rho, scene.h, T=scene.T, fixed=scene.fixed, tool_p=scene.tool_p,
+                stream=stream)
+        s.set_physics(**scene.phys)
+        s.set_correctors(**scene.corr)
+        if scene.joco:
+            s.set_johnson_cook(**scene.joco)
+        s.set_thermal_workpiece(**scene.trml_wp)
+        s.set_thermal_tool(**scene.trml_tool)
+        opts = dict(scene.options)
+        opts.update(option_overrides)
+        s.set_options(**opts)
+        s.set_grid(scene.grid_bbmin, scene.grid_bbmax, scene.grid_h)
+        s.set_blanking(scene.blank_bbmin, scene.blank_bbmax, scene.blank_vmax)
+        for t in scene.tools:
+            s.add_tool(t.verts, t.tris, t.vel, t.contact_alpha, t.mu, t.algorithm)
+        # main() skips the step at index 0 and then advances the clock once
+        dt = np.float32(scene.dt)
+        s.set_time(float(dt), float(np.float32(0) + dt))
+        return s

@@ -1,0 +1,82 @@
+"""Builds libmfree.so (the C-ABI library) in-tree for sm_100a.
+
+CUDA sources are compiled by nvcc with ``-gencode arch=compute_100a,code=sm_100a``
+(default IEEE division/square root: the cell hash must be bit-exact); host C++
+sources by g++.  Usage: ``python -m iwf_mfree_gpu_3d_b200.build [--force]``.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+BUILD = os.path.join(PKG, "_build")
+LIB = os.path.join(PKG, "libmfree.so")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+CU_SOURCES = ["mfree_sort.cu", "mfree_interact.cu", "mfree_contact.cu", "mfree_host.cu", "mfree_probe.cu"]
+CPP_SOURCES = ["mfree_tool.cpp", "mfree_io.cpp"]
+
+
+def _newer(out: str, deps) -> bool:
+    if not os.path.exists(out):
+        return False
+    t = os.path.getmtime(out)
+    return all(os.path.getmtime(d) <= t for d in deps)
+
+
+def _headers():
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    return hs + [os.path.join(INCLUDE, "mfree.h")]
+
+
+def _compile(src: str, force: bool, verbose_ptxas: bool):
+    name = os.path.basename(src)
+    obj = os.path.join(BUILD, name + ".o")
+    if not force and _newer(obj, [src] + _headers()):
+        return obj, ""
+    if src.endswith(".cu"):
+        cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC,
+               "-c", src, "-o", obj]
+        if verbose_ptxas:
+            cmd.insert(1, "-Xptxas=-v")
+    else:
+        cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-I" + INCLUDE, "-I" + CSRC, "-I" + os.path.join(CUDA_HOME, "include"),
+               "-c", src, "-o", obj]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"compile failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return obj, r.stderr
+
+
+def build(force: bool = False, verbose_ptxas: bool = False) -> str:
+    """Compile and link libmfree.so; returns its path."""
+    os.makedirs(BUILD, exist_ok=True)
+    srcs = [os.path.join(CSRC, s) for s in CU_SOURCES + CPP_SOURCES]
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        results = list(ex.map(lambda s: _compile(s, force, verbose_ptxas), srcs))
+    objs = [o for o, _ in results]
+    if verbose_ptxas:
+        for _, log in results:
+            if log:
+                sys.stderr.write(log)
+    if force or not _newer(LIB, objs):
+        tmp = LIB + ".tmp"
+        cmd = [NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-Xcompiler", "-fPIC"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+        shutil.move(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose_ptxas="-v" in sys.argv))

@@ -1,0 +1,328 @@
+// mfree_contact.cu -- end of the step: rigid-tool contact and the work that
+// follows it for the particles inside a tool box.
+//
+// Reference path replaced (src/leap_frog.cu:173-188):
+//   tool_3d_gpu::update_tool + do_update_tool   tool_3d_gpu.cu:74-99,907-948 (vertices
+//                                               p_init + v t are formed on the fly)
+//   do_compute_contact_forces (spatial hashing, safe) tool_3d_gpu.cu:585-681
+//       establish_contact_by_ray / _by_normal, comp_closest_point,
+//       triangle_ray_intersect                  tool_3d_gpu.cu:101-444
+//   do_compute_contact_forces_n2 (exhaustive)   tool_3d_gpu.cu:455-583
+//   tool_forces (atomicAdd)                     tool_3d_gpu.cu:30-69 -- here a
+//                                               fixed-order block reduction
+//   do_material_fric_heat_gen                   actions_gpu.cu:192-220
+//   do_boundary_conditions(_thermal)            actions_gpu.cu:451-487
+//   do_move_tool_particles (blanked tail)       actions_gpu.cu:55-68
+//
+// One thread per particle; only particles inside a tool box do contact work
+// (the pair kernel's epilogue has already finished every other particle).
+#include "mfree_kernels.cuh"
+
+namespace mfree {
+
+namespace {
+
+struct V3 {
+    float x, y, z;
+};
+__device__ __forceinline__ V3 v3(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ V3 operator*(float s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ bool operator==(V3 a, V3 b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+__device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 cross(V3 a, V3 b) {
+    return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y};
+}
+__device__ __forceinline__ float len(V3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ V3 ld(const float4 *p, int i) {
+    float4 v = p[i];
+    return {v.x, v.y, v.z};
+}
+
+// current vertex p_init + v t (do_update_tool)
+__device__ __forceinline__ V3 vert(const ToolDev &T, const float4 *p, int i, float t) {
+    float4 v = p[i];
+    return {v.x + T.vel[0] * t, v.y + T.vel[1] * t, v.z + T.vel[2] * t};
+}
+
+__device__ V3 closest_on_segment(V3 p1, V3 p2, V3 p) {
+    float dx = p1.x - p2.x, dy = p1.y - p2.y, dz = p1.z - p2.z;
+    float ns2 = dx * dx + dy * dy + dz * dz;
+    if (ns2 == 0.f) return p1;
+    float t = ((p2.x - p1.x) * (p.x - p1.x) + (p2.y - p1.y) * (p.y - p1.y) + (p2.z - p1.z) * (p.z - p1.z)) / ns2;
+    if (t > 1.f) return p2;
+    if (t < 0.f) return p1;
+    return (1.f - t) * p1 + t * p2;
+}
+
+// closest point on triangle k and the normal of the feature it lies on
+// (comp_closest_point, tool_3d_gpu.cu:141-212)
+__device__ void closest_point(const ToolDev &T, int k, float t, V3 qp, V3 &cp, V3 &np) {
+    V3 p1 = vert(T, T.p1, k, t), p2 = vert(T, T.p2, k, t), p3 = vert(T, T.p3, k, t);
+    V3 p1p2 = p2 - p1, p1p3 = p3 - p1, pp1 = p1 - qp;
+    float B = dot(p1p3, p1p2), E = dot(p1p2, p1p2), C = dot(p1p3, p1p3);
+    float det = B * B - E * C;
+    float A = dot(p1p3, pp1), D = dot(p1p2, pp1);
+    float t1 = (D * C - A * B) / det, t2 = (A * E - D * B) / det;
+    if (t1 < 0.f) {
+        cp = closest_on_segment(p1, p3, qp);
+        np = cp == p1 ? ld(T.np1, k) : (cp == p3 ? ld(T.np3, k) : ld(T.ne3, k));
+    } else if (t2 < 0.f) {
+        cp = closest_on_segment(p1, p2, qp);
+        np = cp == p1 ? ld(T.np1, k) : (cp == p2 ? ld(T.np2, k) : ld(T.ne1, k));
+    } else if (t1 + t2 > 1.f) {
+        cp = closest_on_segment(p2, p3, qp);
+        np = cp == p2 ? ld(T.np2, k) : (cp == p3 ? ld(T.np3, k) : ld(T.ne2, k));
+    } else {
+        cp = p1 + t1 * p1p2 + t2 * p1p3;
+        np = ld(T.n, k);
+    }
+}
+
+// Moller-Trumbore along +z (triangle_ray_intersect, tool_3d_gpu.cu:248-280)
+__device__ bool ray_z(const ToolDev &T, int k, float t, V3 o, float &tt) {
+    const float EPS = 0.0000001f;
+    V3 v0 = vert(T, T.p1, k, t), v1 = vert(T, T.p2, k, t), v2 = vert(T, T.p3, k, t);
+    V3 e1 = v1 - v0, e2 = v2 - v0;
+    V3 dir = v3(0.f, 0.f, 1.f);
+    V3 h = cross(dir, e2);
+    float a = dot(e1, h);
+    if (a > -EPS && a < EPS) return false;
+    float f = 1.f / a;
+    V3 s = o - v0;
+    float u = f * dot(s, h);
+    if (u < 0.f || u > 1.f) return false;
+    V3 q = cross(s, e1);
+    float v = f * dot(dir, q);
+    if (v < 0.f || u + v > 1.f) return false;
+    tt = f * dot(e2, q);
+    return tt > EPS;
+}
+
+__device__ __forceinline__ void unhash(const ToolDev &T, const ToolClock &B, V3 p, int &ix, int &iy, int &iz) {
+    // (unsigned int) cast of unhash_pos (tool_3d_gpu.cu:101-107), kept inside the grid
+    ix = int(min((unsigned)((p.x - B.bbmin[0]) / T.dx), unsigned(T.nx - 1)));
+    iy = int(min((unsigned)((p.y - B.bbmin[1]) / T.dx), unsigned(T.ny - 1)));
+    iz = int(min((unsigned)((p.z - B.bbmin[2]) / T.dx), unsigned(T.nz - 1)));
+}
+
+// +z ray parity over the tri-grid column (establish_contact_by_ray, :382-444)
+__device__ bool inside_by_ray(const ToolDev &T, const ToolClock &B, float t, V3 qp) {
+    int ix, iy, iz;
+    unhash(T, B, qp, ix, iy, iz);
+    unsigned ni = 0;
+    for (; iz < T.nz; ++iz) {
+        const int box = (ix * T.ny + iy) * T.nz + iz;
+        for (int k = T.cells[box]; k < T.cells[box + 1]; k++) {
+            float tt;
+            if (ray_z(T, k, t, qp, tt)) {
+                V3 ip = qp + tt * v3(0.f, 0.f, 1.f);
+                float lox = B.bbmin[0] + ix * T.dx, loy = B.bbmin[1] + iy * T.dx, loz = B.bbmin[2] + iz * T.dx;
+                float hix = B.bbmin[0] + (ix + 1) * T.dx, hiy = B.bbmin[1] + (iy + 1) * T.dx,
+                      hiz = B.bbmin[2] + (iz + 1) * T.dx;
+                if (lox <= ip.x && ip.x < hix && loy <= ip.y && ip.y < hiy && loz <= ip.z && ip.z < hiz) ni++;
+            }
+        }
+    }
+    return (ni % 2) != 0;
+}
+
+// closest triangle by expanding shells until one is non-empty, plus one more
+// shell (establish_contact_by_normal, :282-380); bounded by the grid size
+__device__ void closest_by_shells(const ToolDev &T, const ToolClock &B, float t, V3 qp, V3 &cp, V3 &nrm,
+                                  DevClock *clk) {
+    int ix, iy, iz;
+    unhash(T, B, qp, ix, iy, iz);
+    float md = __int_as_float(0x7f800000);  // DBL_MAX stored in a float
+    cp = qp;
+    nrm = v3(0.f, 0.f, 0.f);
+    int box = (ix * T.ny + iy) * T.nz + iz;
+    bool empty_so_far = T.cells[box] == T.cells[box + 1];
+    for (int k = T.cells[box]; k < T.cells[box + 1]; k++) {
+        V3 c, n;
+        closest_point(T, k, t, qp, c, n);
+        V3 d = c - qp;
+        float dd = dot(d, d);
+        if (dd < md) { md = dd; cp = c; nrm = n; }
+    }
+    const int cap = max(T.nx, max(T.ny, T.nz)) + 2;
+    bool all_done = false;
+    int off = 1;
+    for (; off <= cap; ) {
+        const int li = max(ix - off, 0), lj = max(iy - off, 0), lk = max(iz - off, 0);
+        const int hi = min(ix + off + 1, T.nx), hj = min(iy + off + 1, T.ny), hk = min(iz + off + 1, T.nz);
+        for (int a = li; a < hi; a++)
+            for (int b = lj; b < hj; b++)
+                for (int c = lk; c < hk; c++) {
+                    bool on = a == li || a == hi - 1 || b == lj || b == hj - 1 || c == lk || c == hk - 1;
+                    if (!on) continue;
+                    const int bx = (a * T.ny + b) * T.nz + c;
+                    for (int k = T.cells[bx]; k < T.cells[bx + 1]; k++) {
+                        empty_so_far = false;
+                        V3 cc, n;
+                        closest_point(T, k, t, qp, cc, n);
+                        V3 d = cc - qp;
+                        float dd = dot(d, d);
+                        if (dd < md) { md = dd; cp = cc; nrm = n; }
+                    }
+                }
+        if (all_done) break;
+        off++;
+        if (!empty_so_far) all_done = true;
+    }
+    if (off > cap) atomicAdd(&clk->contact_cap, 1ull);
+}
+
+}  // namespace
+
+// one thread per particle; particles of the blanked tail only translate if
+// they are tool particles
+__global__ void __launch_bounds__(256) k_finalize(StepArgs a) {
+    const Params &P = a.p;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int N = a.clk->n_active;
+    const bool rec = a.clk->record != 0;
+    const State &S = a.b;
+    float fsum[MAX_TOOLS][3];
+    if (rec)
+        for (int k = 0; k < P.num_tools; k++) fsum[k][0] = fsum[k][1] = fsum[k][2] = 0.f;
+    do {
+        if (i >= P.n_init) break;
+        if (i >= N) {
+            const float4 fc = S.fc4[i];
+            if (fc.w == 1.f) {
+                float4 pos = S.pos4[i];
+                if (P.precision) {
+                    float4 lo = S.lo4[i];
+                    acc_comp(pos.x, lo.x, P.dt, P.tool0_vel[0]);
+                    acc_comp(pos.y, lo.y, P.dt, P.tool0_vel[1]);
+                    acc_comp(pos.z, lo.z, P.dt, P.tool0_vel[2]);
+                    S.lo4[i] = lo;
+                } else {
+                    pos.x = fmaf(P.tool0_vel[0], P.dt, pos.x);
+                    pos.y = fmaf(P.tool0_vel[1], P.dt, pos.y);
+                    pos.z = fmaf(P.tool0_vel[2], P.dt, pos.z);
+                }
+                S.pos4[i] = pos;
+            }
+            break;
+        }
+        float4 pos = S.pos4[i];
+        float4 fc = S.fc4[i];
+        if (fc.w == 1.f) break;  // tool particle
+        if (!contact_candidate(a, pos.x, pos.y, pos.z)) break;
+        const float t = a.clk->t;
+        const float dt = P.dt;
+        float4 vel = S.vel4[i], ft = S.ft4[i];
+        V3 qp = v3(pos.x, pos.y, pos.z);
+        V3 n_last = v3(0.f, 0.f, 0.f);
+        for (int k = 0; k < P.num_tools; k++) {
+            if (!in_tool_box(a, k, pos.x, pos.y, pos.z)) continue;
+            const ToolDev &T = a.tools[k];
+            const ToolClock &B = a.clk->tool[k];
+            V3 cp, n;
+            if (T.hashed) {
+                if (!inside_by_ray(T, B, t, qp)) continue;
+                closest_by_shells(T, B, t, qp, cp, n, a.clk);
+            } else {
+                float md = 3.402823466e+38f;  // FLT_MAX
+                cp = qp;
+                n = v3(0.f, 0.f, 0.f);
+                for (int kk = 0; kk < T.num_tris; kk++) {
+                    V3 c, nn;
+                    closest_point(T, kk, t, qp, c, nn);
+                    V3 d = c - qp;
+                    float dd = dot(d, d);
+                    if (dd < md) { md = dd; cp = c; n = nn; }
+                }
+                if (dot(cp - qp, n) > 0.f) continue;
+            }
+            const float gN = dot(qp - cp, n);
+            V3 fN = T.alpha * ((1.f / (dt * dt)) * ((-P.mass * gN) * n));
+            V3 fT = v3(0.f, 0.f, 0.f);
+            if (T.mu != 0.f) {
+                V3 vm = P.friction_tool_vel ? v3(T.vel[0], T.vel[1], T.vel[2]) : v3(0.f, 0.f, 0.f);
+                V3 v = v3(vel.x, vel.y, vel.z) - vm;
+                V3 vr = v3(v.x - v.x * n.x, v.y - v.y * n.y, v.z - v.z * n.z);
+                V3 kde = (1.f / dt) * ((T.alpha * P.mass) * vr);
+                float fy = T.mu * len(fN);
+                V3 fs = v3(ft.x, ft.y, ft.z) - kde;
+                float lfs = len(fs);
+                fT = lfs > fy ? (fy / lfs) * fs : fs;
+            }
+            fc.x = fN.x; fc.y = fN.y; fc.z = fN.z;
+            ft.x = fT.x; ft.y = fT.y; ft.z = fT.z;
+            n_last = n;
+            if (rec) {
+                fsum[k][0] += fN.x + fT.x;
+                fsum[k][1] += fN.y + fT.y;
+                fsum[k][2] += fN.z + fT.z;
+            }
+        }
+        // friction heat (do_material_fric_heat_gen) with the first tool's velocity
+        float4 sb = S.sb4[i];
+        float T = sb.z;
+        if (P.fric_heat) {
+            const float fm = sqrtf(ft.x * ft.x + ft.y * ft.y + ft.z * ft.z);
+            if (fm != 0.f) {
+                const float dx = vel.x - P.tool0_vel[0], dy = vel.y - P.tool0_vel[1], dz = vel.z - P.tool0_vel[2];
+                const float dn = dx * n_last.x + dy * n_last.y + dz * n_last.z;
+                const float rx = dx - dn, ry = dy - dn, rz = dz - dn;
+                const float vm = sqrtf(rx * rx + ry * ry + rz * rz);
+                T += P.wp_eta * dt * fm * vm / (P.wp_cp * P.mass);
+            }
+        }
+        // boundary conditions
+        const float fixed = S.dsb4[i].w;
+        if (fixed != 0.f) {
+            const float4 bc = S.bc4[i];
+            vel.x = bc.x; vel.y = bc.y; vel.z = bc.z;
+            fc.x = fc.y = fc.z = 0.f;
+            float4 da = S.da4[i], dv = S.dv4[i];
+            da.x = da.y = da.z = 0.f;
+            dv.x = dv.y = dv.z = 0.f;
+            S.da4[i] = da;
+            S.dv4[i] = dv;
+            if (P.precision) {
+                float4 lo = S.lo4[i], lob = S.lo4b[i];
+                lo.w = 0.f; lob.x = lob.y = 0.f;
+                S.lo4[i] = lo;
+                S.lo4b[i] = lob;
+            }
+        }
+        if (P.thermal && fixed == 1.f) T = P.wp_Tinit;
+        sb.z = T;
+        S.sb4[i] = sb;
+        S.vel4[i] = vel;
+        S.fc4[i] = fc;
+        S.ft4[i] = ft;
+        if (P.diagnostics) a.s.nrm[i] = make_float4(n_last.x, n_last.y, n_last.z, 0.f);
+    } while (false);
+    if (!rec) return;
+    // fixed-order block reduction of the tool forces
+    __shared__ float red[8][3 * MAX_TOOLS];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < P.num_tools; k++)
+        for (int d = 0; d < 3; d++) {
+            float v = (i < P.n_init && i < N) ? fsum[k][d] : 0.f;
+            for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) red[warp][3 * k + d] = v;
+        }
+    __syncthreads();
+    if (threadIdx.x < 3 * P.num_tools) {
+        float s = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w][threadIdx.x];
+        a.s.force_part[size_t(blockIdx.x) * (3 * MAX_TOOLS) + threadIdx.x] = s;
+    }
+}
+
+__global__ void k_force_final(StepArgs a, int num_blocks, float *out) {
+    const int c = threadIdx.x;
+    if (c >= 3 * a.p.num_tools || !a.clk->record) return;
+    float s = 0.f;
+    for (int b = 0; b < num_blocks; b++) s += a.s.force_part[size_t(b) * (3 * MAX_TOOLS) + c];
+    out[c] = s;
+}
+
+}  // namespace mfree

@@ -1,0 +1,1080 @@
+// mfree_host.cu -- the C ABI (include/mfree.h): context, device memory, step
+// orchestration and state import/export.
+//
+// Reference host path replaced: particle_gpu construction (particle_gpu.cu:20-117),
+// the constant uploads (actions_gpu.cu:659-710, interactions_gpu.cu:552-608,
+// tool_3d_gpu.cu:683-812), the grid and blanking objects (grid_gpu_base.cu:237-273,
+// blanking.cpp), leap_frog::step (leap_frog.cu:121-195) and the process globals
+// of mfree_gpu_3d.cpp:41-48.
+//
+// A step is 11 kernels on one stream with no host synchronisation (N lives on
+// the device), so it can also be captured once into a CUDA graph and replayed.
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "mfree.h"
+#include "mfree_kernels.cuh"
+#include "mfree_tool.h"
+
+using namespace mfree;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CUDA_TRY(x)                                                                        \
+    do {                                                                                   \
+        cudaError_t e_ = (x);                                                              \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(e_ == cudaErrorMemoryAllocation ? MFREE_ERR_OOM : MFREE_ERR_CUDA,  \
+                        std::string(#x) + ": " + cudaGetErrorString(e_));                 \
+    } while (0)
+
+struct DevTool {
+    HostTool host;
+    int algorithm = MFREE_CONTACT_HASHED;
+    float vel[3] = {0, 0, 0};
+    float alpha = 0.1f, mu = 0.f;
+    float birth = -3.402823466e+38f, death = 3.402823466e+38f;
+    float4 *d_tri = nullptr;  // 10 arrays of float4, back to back
+    int *d_cells = nullptr;
+    int ntri_dev = 0;
+};
+
+}  // namespace
+
+struct mfree_ctx {
+    int n_init = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int device = 0, num_sms = 148;
+    // host-side configuration
+    mfree_phys phys{};
+    mfree_corr corr{};
+    mfree_joco joco{};
+    mfree_trml twp{}, ttool{};
+    mfree_options opt{};
+    bool plastic = false;
+    bool grid_set = false;
+    float g_bbmin[3], g_bbmax[3], g_dx = 0.f, g_vel[3] = {0, 0, 0};
+    long nx = 0, ny = 0, nz = 0, num_cell = 0;
+    bool blank_set = false;
+    float b_min[3], b_max[3], b_vel[3] = {0, 0, 0}, b_vmax = 0.f;
+    float dt = 0.f, t = 0.f;
+    bool time_set = false;
+    std::vector<std::unique_ptr<DevTool>> tools;
+    // device memory
+    State st[2]{};
+    int cur = 0;
+    Records rec{};
+    Scratch scr{};
+    DevClock *d_clk = nullptr;
+    float *d_forces = nullptr;
+    size_t scratch_cells = 0;  // num_cell the scratch was sized for
+    std::vector<void *> allocs, scratch_allocs;
+    bool clock_dirty = true;  // host-side scalars changed: rewrite the device clock
+    bool pending = false;     // a step has run since the clock was written
+    long long steps = 0;
+    // per-kernel timing (eager steps)
+    bool timing = false;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> tev;
+    std::vector<cudaEvent_t> event_pool;
+    double kernel_ms[MFREE_NUM_KERNELS] = {0};
+    int kernel_n[MFREE_NUM_KERNELS] = {0};
+    cudaEvent_t timer[2] = {nullptr, nullptr};
+    // graphs, one per state parity
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int graph_record_every = -1;
+    bool graph_valid = false;
+};
+
+namespace {
+
+template <class T> int dalloc(mfree_ctx *c, T **p, size_t n, std::vector<void *> &list) {
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) return fail(MFREE_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    list.push_back(q);
+    *p = (T *)q;
+    (void)c;
+    return MFREE_OK;
+}
+
+void free_list(std::vector<void *> &l) {
+    for (void *p : l) cudaFree(p);
+    l.clear();
+}
+
+void invalidate_graphs(mfree_ctx *c) {
+    for (auto &g : c->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    c->graph_valid = false;
+}
+
+int default_lpp() { return 8; }
+
+Params make_params(const mfree_ctx *c) {
+    Params P{};
+    P.mass = c->phys.mass;
+    P.K = c->phys.K;
+    P.G = c->phys.G;
+    P.rho0 = c->phys.rho0;
+    {
+        float c0 = std::sqrt(c->phys.rho0 != 0.f ? c->phys.K / c->phys.rho0 : 0.f);
+        P.c0sq = c0 * c0;
+    }
+    P.wdeltap = c->corr.wdeltap;
+    P.stresseps = c->corr.stresseps;
+    P.xspheps = c->corr.xspheps;
+    P.av_alpha = c->corr.alpha;
+    P.av_beta = c->corr.beta;
+    P.av_eta = c->corr.eta;
+    P.wp_alpha = c->twp.alpha;
+    P.wp_cp = c->twp.cp;
+    P.wp_tq = c->twp.tq;
+    P.wp_Tinit = c->twp.T_init;
+    P.wp_eta = c->twp.eta;
+    P.tool_alpha = c->ttool.alpha;
+    P.thermal = (c->twp.alpha != 0.f || c->ttool.alpha != 0.f) ? 1 : 0;
+    P.fric_heat = c->twp.eta != 0.f ? 1 : 0;
+    P.jc_A = c->joco.A;
+    P.jc_B = c->joco.B;
+    P.jc_C = c->joco.C;
+    P.jc_n = c->joco.n;
+    P.jc_m = c->joco.m;
+    P.jc_Tmelt = c->joco.Tmelt;
+    P.jc_Tref = c->joco.Tref;
+    P.jc_epsdot_ref = c->joco.eps_dot_ref;
+    P.jc_clamp = c->joco.clamp_temp;
+    P.plastic = c->plastic ? 1 : 0;
+    P.max_secant_iter = c->opt.max_secant_iter > 0 ? c->opt.max_secant_iter : 100;
+    P.cspm = c->opt.cspm;
+    P.conduction = c->opt.conduction;
+    P.precision = c->opt.precision;
+    P.diagnostics = c->opt.diagnostics;
+    P.friction_tool_vel = c->opt.friction_tool_vel;
+    P.gnx = int(c->nx);
+    P.gny = int(c->ny);
+    P.gnz = int(c->nz);
+    P.num_cell = int(c->num_cell);
+    P.gdx = c->g_dx;
+    P.grid_moving = (c->g_vel[0] != 0.f || c->g_vel[1] != 0.f || c->g_vel[2] != 0.f) ? 1 : 0;
+    for (int d = 0; d < 3; d++) {
+        P.grid_vel[d] = c->g_vel[d];
+        P.grid_min0[d] = c->g_bbmin[d];
+        P.blank_min0[d] = c->b_min[d];
+        P.blank_max0[d] = c->b_max[d];
+        P.blank_vel[d] = c->b_vel[d];
+    }
+    P.blank_on = c->blank_set ? 1 : 0;
+    P.vmax2 = c->b_vmax * c->b_vmax;
+    P.dt = c->dt;
+    P.n_init = c->n_init;
+    P.num_tools = int(c->tools.size());
+    for (int d = 0; d < 3; d++) P.tool0_vel[d] = c->tools.empty() ? 0.f : c->tools[0]->vel[d];
+    P.record_every = 0;
+    return P;
+}
+
+int hash_blocks(const mfree_ctx *c) { return (c->n_init + HASH_BLOCK - 1) / HASH_BLOCK; }
+int scan_tiles(const mfree_ctx *c) { return int((c->num_cell + 1 + SCAN_TILE - 1) / SCAN_TILE); }
+
+StepArgs make_args(mfree_ctx *c) {
+    StepArgs a{};
+    a.p = make_params(c);
+    a.a = c->st[c->cur];
+    a.b = c->st[c->cur ^ 1];
+    a.r = c->rec;
+    a.s = c->scr;
+    a.clk = c->d_clk;
+    for (size_t k = 0; k < c->tools.size() && k < size_t(MAX_TOOLS); k++) {
+        const DevTool &t = *c->tools[k];
+        ToolDev &d = a.tools[k];
+        const int n = t.ntri_dev;
+        d.p1 = t.d_tri;
+        d.p2 = t.d_tri + n;
+        d.p3 = t.d_tri + 2 * n;
+        d.n = t.d_tri + 3 * n;
+        d.np1 = t.d_tri + 4 * n;
+        d.np2 = t.d_tri + 5 * n;
+        d.np3 = t.d_tri + 6 * n;
+        d.ne1 = t.d_tri + 7 * n;
+        d.ne2 = t.d_tri + 8 * n;
+        d.ne3 = t.d_tri + 9 * n;
+        d.cells = t.d_cells;
+        d.num_tris = t.host.boxed.empty() ? 0 : n;
+        d.nx = t.host.nx;
+        d.ny = t.host.ny;
+        d.nz = t.host.nz;
+        d.dx = t.host.dx;
+        for (int q = 0; q < 3; q++) d.vel[q] = t.vel[q];
+        d.alpha = t.alpha;
+        d.mu = t.mu;
+        d.hashed = t.algorithm == MFREE_CONTACT_HASHED ? 1 : 0;
+        d.birth = t.birth;
+        d.death = t.death;
+    }
+    return a;
+}
+
+// scratch that depends on the grid size
+int ensure_scratch(mfree_ctx *c) {
+    if (c->scratch_cells == size_t(c->num_cell) && !c->scratch_allocs.empty()) return MFREE_OK;
+    free_list(c->scratch_allocs);
+    auto &L = c->scratch_allocs;
+    int st;
+    if ((st = dalloc(c, &c->scr.count, c->num_cell + 1, L))) return st;
+    if ((st = dalloc(c, &c->scr.first, c->num_cell + 2 + SCAN_TILE, L))) return st;
+    if ((st = dalloc(c, &c->scr.tile_sum, scan_tiles(c) + 1, L))) return st;
+    CUDA_TRY(cudaMemsetAsync(c->scr.count, 0, sizeof(int) * (c->num_cell + 1), c->stream));
+    c->scratch_cells = size_t(c->num_cell);
+    invalidate_graphs(c);
+    return MFREE_OK;
+}
+
+int write_clock(mfree_ctx *c) {
+    DevClock h{};
+    h.t = c->t;
+    h.pending = 0;
+    h.n_active = c->n_init;
+    h.record = 0;
+    h.step_index = c->steps;
+    for (int d = 0; d < 3; d++) {
+        h.blank_min[d] = c->b_min[d];
+        h.blank_max[d] = c->b_max[d];
+        h.grid_min[d] = c->g_bbmin[d];
+    }
+    for (size_t k = 0; k < c->tools.size(); k++)
+        for (int d = 0; d < 3; d++) {
+            h.tool[k].bbmin[d] = c->tools[k]->host.bbmin[d];
+            h.tool[k].bbmax[d] = c->tools[k]->host.bbmax[d];
+        }
+    // keep the device counters
+    DevClock old{};
+    CUDA_TRY(cudaMemcpyAsync(&old, c->d_clk, sizeof(DevClock), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    h.secant_failures = old.secant_failures;
+    h.out_of_grid = old.out_of_grid;
+    h.contact_cap = old.contact_cap;
+    h.nan_blanked = old.nan_blanked;
+    h.n_active = old.n_active ? old.n_active : c->n_init;
+    CUDA_TRY(cudaMemcpyAsync(c->d_clk, &h, sizeof(DevClock), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->clock_dirty = false;
+    c->pending = false;
+    return MFREE_OK;
+}
+
+int ready(mfree_ctx *c) {
+    if (!c->grid_set) return fail(MFREE_ERR_ARG, "mfree_set_grid must be called before stepping");
+    if (!c->time_set || !(c->dt > 0.f)) return fail(MFREE_ERR_ARG, "mfree_set_time must set dt > 0 before stepping");
+    if (c->phys.mass <= 0.f || c->phys.rho0 <= 0.f) return fail(MFREE_ERR_ARG, "mfree_set_physics: mass and rho0 must be > 0");
+    if (c->tools.size() > size_t(MAX_TOOLS)) return fail(MFREE_ERR_ARG, "too many tools");
+    int lpp = c->opt.lanes_per_particle;
+    if (lpp != 0 && lpp != 4 && lpp != 8 && lpp != 16 && lpp != 32)
+        return fail(MFREE_ERR_ARG, "lanes_per_particle must be 0, 4, 8, 16 or 32");
+    if (c->opt.conduction < 0 || c->opt.conduction > 2) return fail(MFREE_ERR_ARG, "bad conduction mode");
+    int st = ensure_scratch(c);
+    if (st) return st;
+    if (c->clock_dirty) return write_clock(c);
+    return MFREE_OK;
+}
+
+cudaEvent_t pooled_event(mfree_ctx *c) {
+    if (!c->event_pool.empty()) {
+        cudaEvent_t e = c->event_pool.back();
+        c->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// the kernels of one step; record_mode as k_clock
+int enqueue_step(mfree_ctx *c, int record_mode, int record_every, bool timed = false) {
+    StepArgs a = make_args(c);
+    a.p.record_every = record_every;
+    cudaStream_t s = c->stream;
+    const int hb = hash_blocks(c), tiles = scan_tiles(c);
+    const int nb = (c->n_init + 255) / 256;
+    const int lpp = c->opt.lanes_per_particle ? c->opt.lanes_per_particle : default_lpp();
+    cudaError_t le = cudaSuccess;
+    auto run = [&](int id, auto &&launch) {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (timed) {
+            e0 = pooled_event(c);
+            e1 = pooled_event(c);
+            cudaEventRecord(e0, s);
+        }
+        launch();
+        if (timed) {
+            cudaEventRecord(e1, s);
+            c->tev.push_back({id, {e0, e1}});
+        }
+    };
+    run(0, [&] { k_clock<<<1, 32, 0, s>>>(a, record_mode); });
+    run(1, [&] { k_hash<<<hb, HASH_BLOCK, 0, s>>>(a); });
+    run(2, [&] { k_scan_reduce<<<tiles, SCAN_THREADS, 0, s>>>(a); });
+    run(3, [&] { k_scan_top<<<1, 1024, 0, s>>>(a, tiles, hb); });
+    run(4, [&] { k_scan_down<<<tiles, SCAN_THREADS, 0, s>>>(a); });
+    run(5, [&] { k_scatter<<<hb, HASH_BLOCK, 0, s>>>(a); });
+    run(6, [&] { k_cell_fixup<<<int((c->num_cell + 255) / 256), 256, 0, s>>>(a); });
+    run(7, [&] { launch_gather_predict(a, nb, s); });
+    run(8, [&] { le = launch_interact(a, lpp, interact_grid_size(lpp, c->n_init, c->num_sms), s); });
+    if (le != cudaSuccess) return fail(MFREE_ERR_CUDA, std::string("pair kernel launch: ") + cudaGetErrorString(le));
+    run(9, [&] { k_finalize<<<nb, 256, 0, s>>>(a); });
+    if (!c->tools.empty()) run(10, [&] { k_force_final<<<1, 32, 0, s>>>(a, nb, c->d_forces); });
+    CUDA_TRY(cudaGetLastError());
+    return MFREE_OK;
+}
+
+int copy_field_raw(mfree_ctx *c, const float4 *src, std::vector<float4> &dst) {
+    dst.resize(c->n_init);
+    CUDA_TRY(cudaMemcpyAsync(dst.data(), src, sizeof(float4) * c->n_init, cudaMemcpyDeviceToHost, c->stream));
+    return MFREE_OK;
+}
+
+}  // namespace
+
+// ======================================================================= ABI
+extern "C" {
+
+const char *mfree_last_error(void) { return g_err.c_str(); }
+
+int mfree_create(int n, const float *pos4, const float *vel4, const float *rho, const float *T, const float *h,
+                 const float *fixed, const float *tool_p, void *stream, mfree_ctx **out) {
+    if (!out || n <= 0 || !pos4 || !vel4 || !rho || !h) return fail(MFREE_ERR_ARG, "mfree_create: bad arguments");
+    *out = nullptr;
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    auto c = std::make_unique<mfree_ctx>();
+    c->n_init = n;
+    c->stream = (cudaStream_t)stream;
+    if (!c->stream) {  // own stream: graph capture is not allowed on the legacy default stream
+        CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    c->device = dev;
+    CUDA_TRY(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev));
+    c->opt.max_secant_iter = 100;
+    auto &L = c->allocs;
+    int st;
+    for (int b = 0; b < 2; b++) {
+        State &S = c->st[b];
+        float4 **f[] = {&S.pos4, &S.vel4, &S.sa4, &S.sb4, &S.da4, &S.dv4, &S.dsa4, &S.dsb4,
+                        &S.fc4, &S.ft4, &S.bc4, &S.lo4, &S.lo4b};
+        for (auto p : f)
+            if ((st = dalloc(c.get(), p, n, L))) return st;
+    }
+    float4 **r[] = {&c->rec.P, &c->rec.V, &c->rec.A, &c->rec.B, &c->rec.R, &c->rec.C};
+    for (auto p : r)
+        if ((st = dalloc(c.get(), p, n, L))) return st;
+    if ((st = dalloc(c.get(), &c->scr.key, n, L))) return st;
+    if ((st = dalloc(c.get(), &c->scr.key_sorted, n, L))) return st;
+    if ((st = dalloc(c.get(), &c->scr.perm, n, L))) return st;
+    if ((st = dalloc(c.get(), &c->scr.blank_block, (n + HASH_BLOCK - 1) / HASH_BLOCK + 1, L))) return st;
+    if ((st = dalloc(c.get(), &c->scr.nnb, n, L))) return st;
+    if ((st = dalloc(c.get(), &c->scr.pos_half, n, L))) return st;
+    if ((st = dalloc(c.get(), &c->scr.nrm, n, L))) return st;
+    if ((st = dalloc(c.get(), &c->scr.force_part, size_t((n + 255) / 256) * 3 * MAX_TOOLS, L))) return st;
+    if ((st = dalloc(c.get(), &c->d_clk, 1, L))) return st;
+    if ((st = dalloc(c.get(), &c->d_forces, 3 * MAX_TOOLS, L))) return st;
+    CUDA_TRY(cudaMemsetAsync(c->d_clk, 0, sizeof(DevClock), c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->d_forces, 0, sizeof(float) * 3 * MAX_TOOLS, c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->scr.nnb, 0, sizeof(int) * n, c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->scr.pos_half, 0, sizeof(float4) * n, c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->scr.nrm, 0, sizeof(float4) * n, c->stream));
+    // initial state, reference constructor semantics (zeros except the given fields)
+    std::vector<float4> hp(n), hv(n), hz(n, make_float4(0, 0, 0, 0)), hsb(n), hdsb(n), hfc(n), hft(n), hbc(n);
+    std::vector<int> perm(n);
+    for (int i = 0; i < n; i++) {
+        hp[i] = make_float4(pos4[4 * i], pos4[4 * i + 1], pos4[4 * i + 2], h[i]);
+        hv[i] = make_float4(vel4[4 * i], vel4[4 * i + 1], vel4[4 * i + 2], rho[i]);
+        hsb[i] = make_float4(0.f, 0.f, T ? T[i] : 0.f, 0.f);
+        hdsb[i] = make_float4(0.f, 0.f, 0.f, fixed ? fixed[i] : 0.f);
+        hfc[i] = make_float4(0.f, 0.f, 0.f, tool_p ? tool_p[i] : 0.f);
+        hft[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        int id = i;
+        float idf;
+        std::memcpy(&idf, &id, 4);
+        hbc[i] = make_float4(0.f, 0.f, 0.f, idf);
+        perm[i] = i;
+    }
+    State &S = c->st[0];
+    auto up = [&](float4 *d, const std::vector<float4> &v) {
+        return cudaMemcpyAsync(d, v.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, c->stream);
+    };
+    CUDA_TRY(up(S.pos4, hp));
+    CUDA_TRY(up(S.vel4, hv));
+    CUDA_TRY(up(S.sa4, hz));
+    CUDA_TRY(up(S.sb4, hsb));
+    CUDA_TRY(up(S.da4, hz));
+    CUDA_TRY(up(S.dv4, hz));
+    CUDA_TRY(up(S.dsa4, hz));
+    CUDA_TRY(up(S.dsb4, hdsb));
+    CUDA_TRY(up(S.fc4, hfc));
+    CUDA_TRY(up(S.ft4, hft));
+    CUDA_TRY(up(S.bc4, hbc));
+    CUDA_TRY(up(S.lo4, hz));
+    CUDA_TRY(up(S.lo4b, hz));
+    for (auto p : r) CUDA_TRY(up(*p, hz));
+    CUDA_TRY(cudaMemcpyAsync(c->scr.perm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->scr.key_sorted, 0, sizeof(int) * n, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    *out = c.release();
+    return MFREE_OK;
+}
+
+int mfree_destroy(mfree_ctx *c) {
+    if (!c) return MFREE_OK;
+    cudaStreamSynchronize(c->stream);
+    invalidate_graphs(c);
+    for (auto &t : c->tools) {
+        if (t->d_tri) cudaFree(t->d_tri);
+        if (t->d_cells) cudaFree(t->d_cells);
+    }
+    free_list(c->scratch_allocs);
+    free_list(c->allocs);
+    for (auto &t : c->tev) {
+        cudaEventDestroy(t.second.first);
+        cudaEventDestroy(t.second.second);
+    }
+    for (auto e : c->event_pool) cudaEventDestroy(e);
+    for (auto e : c->timer)
+        if (e) cudaEventDestroy(e);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return MFREE_OK;
+}
+
+int mfree_set_physics(mfree_ctx *c, const mfree_phys *p) {
+    if (!c || !p) return fail(MFREE_ERR_ARG, "null argument");
+    if (p->mass == 0.f || std::isnan(p->mass)) return fail(MFREE_ERR_ARG, "invalid particle mass");
+    c->phys = *p;
+    invalidate_graphs(c);
+    return MFREE_OK;
+}
+int mfree_set_correctors(mfree_ctx *c, const mfree_corr *p) {
+    if (!c || !p) return fail(MFREE_ERR_ARG, "null argument");
+    c->corr = *p;
+    invalidate_graphs(c);
+    return MFREE_OK;
+}
+int mfree_set_johnson_cook(mfree_ctx *c, const mfree_joco *p) {
+    if (!c || !p) return fail(MFREE_ERR_ARG, "null argument");
+    c->joco = *p;
+    c->plastic = true;
+    invalidate_graphs(c);
+    return MFREE_OK;
+}
+int mfree_set_thermal_workpiece(mfree_ctx *c, const mfree_trml *p) {
+    if (!c || !p) return fail(MFREE_ERR_ARG, "null argument");
+    c->twp = *p;
+    invalidate_graphs(c);
+    return MFREE_OK;
+}
+int mfree_set_thermal_tool(mfree_ctx *c, const mfree_trml *p) {
+    if (!c || !p) return fail(MFREE_ERR_ARG, "null argument");
+    c->ttool = *p;
+    invalidate_graphs(c);
+    return MFREE_OK;
+}
+int mfree_set_options(mfree_ctx *c, const mfree_options *o) {
+    if (!c || !o) return fail(MFREE_ERR_ARG, "null argument");
+    c->opt = *o;
+    if (c->opt.max_secant_iter <= 0) c->opt.max_secant_iter = 100;
+    invalidate_graphs(c);
+    return MFREE_OK;
+}
+int mfree_get_options(const mfree_ctx *c, mfree_options *o) {
+    if (!c || !o) return fail(MFREE_ERR_ARG, "null argument");
+    *o = c->opt;
+    return MFREE_OK;
+}
+
+int mfree_set_grid(mfree_ctx *c, const float bbmin[3], const float bbmax[3], float h) {
+    if (!c || !bbmin || !bbmax || !(h > 0.f)) return fail(MFREE_ERR_ARG, "mfree_set_grid: bad arguments");
+    // set_geometry (grid_gpu_base.cu:237-273) in float, as the reference
+    for (int d = 0; d < 3; d++) {
+        c->g_bbmin[d] = float(double(bbmin[d]) - 1e-6);
+        c->g_bbmax[d] = float(double(bbmax[d]) + 1e-6);
+    }
+    float kernel_width = 2.f;
+    c->g_dx = float(double(h * kernel_width) / 2.);
+    float lx = c->g_bbmax[0] - c->g_bbmin[0], ly = c->g_bbmax[1] - c->g_bbmin[1], lz = c->g_bbmax[2] - c->g_bbmin[2];
+    c->nx = long(std::ceil(lx / c->g_dx));
+    c->ny = long(std::ceil(ly / c->g_dx));
+    c->nz = long(std::ceil(lz / c->g_dx));
+    if (c->nx <= 0 || c->ny <= 0 || c->nz <= 0) return fail(MFREE_ERR_ARG, "empty grid");
+    long nc = c->nx * c->ny * c->nz;
+    if (nc >= long(INT_MAX) / 2) return fail(MFREE_ERR_ARG, "grid has too many cells");
+    c->num_cell = nc;
+    c->grid_set = true;
+    c->clock_dirty = true;
+    invalidate_graphs(c);
+    return MFREE_OK;
+}
+int mfree_set_grid_velocity(mfree_ctx *c, const float vel[3]) {
+    if (!c || !vel) return fail(MFREE_ERR_ARG, "null argument");
+    for (int d = 0; d < 3; d++) c->g_vel[d] = vel[d];
+    invalidate_graphs(c);
+    return MFREE_OK;
+}
+int mfree_set_blanking(mfree_ctx *c, const float bbmin[3], const float bbmax[3], const float *bbvel3, float max_vel) {
+    if (!c || !bbmin || !bbmax) return fail(MFREE_ERR_ARG, "null argument");
+    for (int d = 0; d < 3; d++) {
+        c->b_min[d] = bbmin[d];
+        c->b_max[d] = bbmax[d];
+        c->b_vel[d] = bbvel3 ? bbvel3[d] : 0.f;
+    }
+    c->b_vmax = max_vel;
+    c->blank_set = true;
+    c->clock_dirty = true;
+    invalidate_graphs(c);
+    return MFREE_OK;
+}
+int mfree_set_time(mfree_ctx *c, float dt, float t) {
+    if (!c || !(dt > 0.f)) return fail(MFREE_ERR_ARG, "mfree_set_time: dt must be > 0");
+    if (c->pending) {  // bring the host clock in line with the device before overwriting
+        mfree_sync(c);
+    }
+    c->dt = dt;
+    c->t = t;
+    c->time_set = true;
+    c->clock_dirty = true;
+    invalidate_graphs(c);
+    return MFREE_OK;
+}
+int mfree_get_time(const mfree_ctx *c, float *dt, float *t) {
+    if (!c) return fail(MFREE_ERR_ARG, "null argument");
+    if (dt) *dt = c->dt;
+    if (t) *t = c->pending ? c->t + c->dt : c->t;  // main() adds dt after each step
+    return MFREE_OK;
+}
+
+int mfree_add_tool(mfree_ctx *c, const float *verts, int nv, const int *tris, int nt, const float vel[3],
+                   float contact_alpha, float mu, int algorithm, int *tool_index) {
+    if (!c || !verts || !tris || !vel) return fail(MFREE_ERR_ARG, "mfree_add_tool: null argument");
+    if (c->tools.size() >= size_t(MAX_TOOLS)) return fail(MFREE_ERR_ARG, "mfree_add_tool: at most 8 tools");
+    if (algorithm != MFREE_CONTACT_HASHED && algorithm != MFREE_CONTACT_EXHAUSTIVE)
+        return fail(MFREE_ERR_ARG, "mfree_add_tool: unknown contact algorithm");
+    auto t = std::make_unique<DevTool>();
+    std::string err;
+    if (!build_host_tool(t->host, verts, nv, tris, nt, err)) return fail(MFREE_ERR_ARG, "mfree_add_tool: " + err);
+    t->algorithm = algorithm;
+    for (int d = 0; d < 3; d++) t->vel[d] = vel[d];
+    t->alpha = contact_alpha;
+    t->mu = mu;
+    const std::vector<HostTri> &src = algorithm == MFREE_CONTACT_HASHED ? t->host.boxed : t->host.tris;
+    const int n = int(src.size());
+    t->ntri_dev = n;
+    std::vector<float4> h(size_t(10) * std::max(n, 1));
+    auto f4 = [](Vec3f v) { return make_float4(v.x, v.y, v.z, 0.f); };
+    for (int k = 0; k < n; k++) {
+        const HostTri &q = src[k];
+        h[k] = f4(q.p1);
+        h[n + k] = f4(q.p2);
+        h[2 * n + k] = f4(q.p3);
+        h[3 * n + k] = f4(q.n);
+        h[4 * n + k] = f4(q.np1);
+        h[5 * n + k] = f4(q.np2);
+        h[6 * n + k] = f4(q.np3);
+        h[7 * n + k] = f4(q.ne1);
+        h[8 * n + k] = f4(q.ne2);
+        h[9 * n + k] = f4(q.ne3);
+    }
+    CUDA_TRY(cudaMalloc(&t->d_tri, sizeof(float4) * h.size()));
+    CUDA_TRY(cudaMemcpy(t->d_tri, h.data(), sizeof(float4) * h.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMalloc(&t->d_cells, sizeof(int) * t->host.cells.size()));
+    CUDA_TRY(cudaMemcpy(t->d_cells, t->host.cells.data(), sizeof(int) * t->host.cells.size(), cudaMemcpyHostToDevice));
+    c->tools.push_back(std::move(t));
+    if (tool_index) *tool_index = int(c->tools.size()) - 1;
+    c->clock_dirty = true;
+    invalidate_graphs(c);
+    return MFREE_OK;
+}
+int mfree_tool_set_birth_death(mfree_ctx *c, int k, float birth, float death) {
+    if (!c || k < 0 || k >= int(c->tools.size())) return fail(MFREE_ERR_ARG, "bad tool index");
+    c->tools[k]->birth = birth;
+    c->tools[k]->death = death;
+    invalidate_graphs(c);
+    return MFREE_OK;
+}
+int mfree_get_tool_forces(mfree_ctx *c, float *out3) {
+    if (!c || !out3) return fail(MFREE_ERR_ARG, "null argument");
+    if (c->tools.empty()) return MFREE_OK;
+    CUDA_TRY(cudaMemcpyAsync(out3, c->d_forces, sizeof(float) * 3 * c->tools.size(), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return MFREE_OK;
+}
+int mfree_get_tool_info(mfree_ctx *c, int k, int *num_tris, int *num_boxed, int *grid_n3, float *bbmin3,
+                        float *bbmax3, float *cell_dx) {
+    if (!c || k < 0 || k >= int(c->tools.size())) return fail(MFREE_ERR_ARG, "bad tool index");
+    const HostTool &t = c->tools[k]->host;
+    if (num_tris) *num_tris = int(t.tris.size());
+    if (num_boxed) *num_boxed = int(t.boxed.size());
+    if (grid_n3) { grid_n3[0] = t.nx; grid_n3[1] = t.ny; grid_n3[2] = t.nz; }
+    for (int d = 0; d < 3; d++) {
+        if (bbmin3) bbmin3[d] = t.bbmin[d];
+        if (bbmax3) bbmax3[d] = t.bbmax[d];
+    }
+    if (cell_dx) *cell_dx = t.dx;
+    return MFREE_OK;
+}
+int mfree_get_tool_normals(mfree_ctx *c, int k, float *out) {
+    if (!c || !out || k < 0 || k >= int(c->tools.size())) return fail(MFREE_ERR_ARG, "bad tool index");
+    const HostTool &t = c->tools[k]->host;
+    for (size_t i = 0; i < t.tris.size(); i++) {
+        const HostTri &q = t.tris[i];
+        const Vec3f v[7] = {q.n, q.np1, q.np2, q.np3, q.ne1, q.ne2, q.ne3};
+        for (int a = 0; a < 7; a++) {
+            out[i * 21 + a * 3] = v[a].x;
+            out[i * 21 + a * 3 + 1] = v[a].y;
+            out[i * 21 + a * 3 + 2] = v[a].z;
+        }
+    }
+    return MFREE_OK;
+}
+int mfree_get_tool_cells(mfree_ctx *c, int k, int *cells, int *boxed_src) {
+    if (!c || k < 0 || k >= int(c->tools.size())) return fail(MFREE_ERR_ARG, "bad tool index");
+    const HostTool &t = c->tools[k]->host;
+    if (cells) std::memcpy(cells, t.cells.data(), sizeof(int) * t.cells.size());
+    if (boxed_src) std::memcpy(boxed_src, t.boxed_src.data(), sizeof(int) * t.boxed_src.size());
+    return MFREE_OK;
+}
+
+int mfree_step(mfree_ctx *c, int record_forces) {
+    if (!c) return fail(MFREE_ERR_ARG, "null context");
+    int st = ready(c);
+    if (st) return st;
+    if ((st = enqueue_step(c, record_forces ? 1 : 0, 0, c->timing))) return st;
+    c->cur ^= 1;
+    if (c->pending) c->t = c->t + c->dt;
+    c->pending = true;
+    c->steps++;
+    return MFREE_OK;
+}
+
+int mfree_advance(mfree_ctx *c, int nsteps, int record_every, int use_graph) {
+    if (!c || nsteps < 0) return fail(MFREE_ERR_ARG, "bad arguments");
+    int st = ready(c);
+    if (st) return st;
+    if (!use_graph) {
+        for (int k = 0; k < nsteps; k++) {
+            const bool rec = record_every > 0 && (c->steps % record_every) == 0;
+            if ((st = enqueue_step(c, rec ? 1 : 0, 0))) return st;
+            c->cur ^= 1;
+            if (c->pending) c->t = c->t + c->dt;
+            c->pending = true;
+            c->steps++;
+        }
+        return MFREE_OK;
+    }
+    if (!c->graph_valid || c->graph_record_every != record_every) {
+        invalidate_graphs(c);
+        for (int parity = 0; parity < 2; parity++) {
+            const int keep = c->cur;
+            c->cur = parity;
+            cudaGraph_t g = nullptr;
+            CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            int e = enqueue_step(c, 2, record_every);
+            cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+            c->cur = keep;
+            if (e) {
+                if (g) cudaGraphDestroy(g);
+                return e;
+            }
+            if (ce != cudaSuccess) return fail(MFREE_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+            cudaError_t ie = cudaGraphInstantiate(&c->graph[parity], g, 0);
+            cudaGraphDestroy(g);
+            if (ie != cudaSuccess) return fail(MFREE_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+        }
+        c->graph_valid = true;
+        c->graph_record_every = record_every;
+    }
+    for (int k = 0; k < nsteps; k++) {
+        CUDA_TRY(cudaGraphLaunch(c->graph[c->cur], c->stream));
+        c->cur ^= 1;
+        if (c->pending) c->t = c->t + c->dt;
+        c->pending = true;
+        c->steps++;
+    }
+    return MFREE_OK;
+}
+
+int mfree_set_kernel_timing(mfree_ctx *c, int on) {
+    if (!c) return fail(MFREE_ERR_ARG, "null context");
+    c->timing = on != 0;
+    return MFREE_OK;
+}
+
+int mfree_get_kernel_times(mfree_ctx *c, double *ms, int *launches) {
+    if (!c) return fail(MFREE_ERR_ARG, "null context");
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (auto &t : c->tev) {
+        float x = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&x, t.second.first, t.second.second));
+        c->kernel_ms[t.first] += x;
+        c->kernel_n[t.first] += 1;
+        c->event_pool.push_back(t.second.first);
+        c->event_pool.push_back(t.second.second);
+    }
+    c->tev.clear();
+    for (int k = 0; k < MFREE_NUM_KERNELS; k++) {
+        if (ms) ms[k] = c->kernel_ms[k];
+        if (launches) launches[k] = c->kernel_n[k];
+        c->kernel_ms[k] = 0.0;
+        c->kernel_n[k] = 0;
+    }
+    return MFREE_OK;
+}
+
+int mfree_timer_start(mfree_ctx *c) {
+    if (!c) return fail(MFREE_ERR_ARG, "null context");
+    for (auto &e : c->timer)
+        if (!e) CUDA_TRY(cudaEventCreate(&e));
+    CUDA_TRY(cudaEventRecord(c->timer[0], c->stream));
+    return MFREE_OK;
+}
+
+int mfree_timer_stop(mfree_ctx *c, double *ms) {
+    if (!c || !ms || !c->timer[0]) return fail(MFREE_ERR_ARG, "timer not started");
+    CUDA_TRY(cudaEventRecord(c->timer[1], c->stream));
+    CUDA_TRY(cudaEventSynchronize(c->timer[1]));
+    float x = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&x, c->timer[0], c->timer[1]));
+    *ms = x;
+    return MFREE_OK;
+}
+
+int mfree_set_device(int device) {
+    CUDA_TRY(cudaSetDevice(device));
+    return MFREE_OK;
+}
+
+int mfree_probe_fp32_peak(double *tflops) {
+    if (!tflops) return fail(MFREE_ERR_ARG, "null argument");
+    int dev = 0, sms = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    *tflops = fp32_peak_probe(sms);
+    if (!(*tflops > 0.0)) return fail(MFREE_ERR_CUDA, "FP32 probe failed");
+    return MFREE_OK;
+}
+
+int mfree_sync(mfree_ctx *c) {
+    if (!c) return fail(MFREE_ERR_ARG, "null context");
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return MFREE_OK;
+}
+
+int mfree_get_counts(const mfree_ctx *c, int *n_active, int *n_init) {
+    if (!c) return fail(MFREE_ERR_ARG, "null context");
+    if (n_init) *n_init = c->n_init;
+    if (n_active) {
+        DevClock h{};
+        CUDA_TRY(cudaMemcpyAsync(&h, c->d_clk, sizeof(DevClock), cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        *n_active = c->steps ? h.n_active : c->n_init;
+    }
+    return MFREE_OK;
+}
+
+int mfree_get_counters(mfree_ctx *c, mfree_counters *o) {
+    if (!c || !o) return fail(MFREE_ERR_ARG, "null argument");
+    DevClock h{};
+    CUDA_TRY(cudaMemcpyAsync(&h, c->d_clk, sizeof(DevClock), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    o->steps = c->steps;
+    o->secant_failures = int64_t(h.secant_failures);
+    o->out_of_grid = int64_t(h.out_of_grid);
+    o->contact_search_cap = int64_t(h.contact_cap);
+    o->nan_blanked = int64_t(h.nan_blanked);
+    return MFREE_OK;
+}
+
+int mfree_field_width(int f) {
+    switch (f) {
+        case MFREE_POS: case MFREE_VEL: case MFREE_VEL_BC: case MFREE_POS_HALF: return 4;
+        case MFREE_S: case MFREE_R: case MFREE_S_T: return 9;
+        case MFREE_FC: case MFREE_FT: case MFREE_NRM: case MFREE_POS_T: case MFREE_VEL_T: return 3;
+        default: return (f >= 0 && f < MFREE_NUM_FIELDS) ? 1 : -1;
+    }
+}
+
+namespace {
+
+// symmetric 6 (xx yy zz xy xz yz) -> GLM column-major 9
+inline void sym_to_9(const float s[6], float *o) {
+    o[0] = s[0]; o[1] = s[3]; o[2] = s[4];
+    o[3] = s[3]; o[4] = s[1]; o[5] = s[5];
+    o[6] = s[4]; o[7] = s[5]; o[8] = s[2];
+}
+
+int get_field_impl(mfree_ctx *c, int f, float *fo, double *dout) {
+    const int n = c->n_init;
+    const State &S = c->st[c->cur];
+    std::vector<float4> A, B, C;
+    int st = 0;
+    const int w = mfree_field_width(f);
+    if (w < 0) return fail(MFREE_ERR_ARG, "unknown field");
+    std::vector<float> tmp(size_t(n) * w);
+    auto put = [&](int i, int k, float v) { tmp[size_t(i) * w + k] = v; };
+    auto ints = [&](const int *dsrc, bool map_hash) -> int {
+        std::vector<int> v(n);
+        CUDA_TRY(cudaMemcpyAsync(v.data(), dsrc, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        for (int i = 0; i < n; i++) {
+            int x = v[i];
+            if (map_hash && x >= int(c->num_cell)) x = INT_MAX;
+            if (fo) std::memcpy(&fo[i], &x, 4);
+            if (dout) dout[i] = double(x);
+        }
+        return MFREE_OK;
+    };
+    switch (f) {
+        case MFREE_POS:
+        case MFREE_VEL: {
+            if ((st = copy_field_raw(c, f == MFREE_POS ? S.pos4 : S.vel4, A))) return st;
+            if (c->opt.precision && dout) {
+                if ((st = copy_field_raw(c, S.lo4, B))) return st;
+                if ((st = copy_field_raw(c, S.lo4b, C))) return st;
+            }
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            for (int i = 0; i < n; i++) {
+                put(i, 0, A[i].x); put(i, 1, A[i].y); put(i, 2, A[i].z); put(i, 3, 0.f);
+            }
+            if (c->opt.precision && dout) {
+                for (int i = 0; i < n; i++) {
+                    double lo[3] = {f == MFREE_POS ? B[i].x : B[i].w, f == MFREE_POS ? B[i].y : C[i].x,
+                                    f == MFREE_POS ? B[i].z : C[i].y};
+                    dout[4 * i] = double(A[i].x) + lo[0];
+                    dout[4 * i + 1] = double(A[i].y) + lo[1];
+                    dout[4 * i + 2] = double(A[i].z) + lo[2];
+                    dout[4 * i + 3] = 0.0;
+                }
+                return MFREE_OK;
+            }
+            break;
+        }
+        case MFREE_VEL_BC:
+            if ((st = copy_field_raw(c, S.bc4, A))) return st;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            for (int i = 0; i < n; i++) { put(i, 0, A[i].x); put(i, 1, A[i].y); put(i, 2, A[i].z); put(i, 3, 0.f); }
+            break;
+        case MFREE_H:
+            if ((st = copy_field_raw(c, S.pos4, A))) return st;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            for (int i = 0; i < n; i++) put(i, 0, A[i].w);
+            break;
+        case MFREE_RHO:
+            if ((st = copy_field_raw(c, S.vel4, A))) return st;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            for (int i = 0; i < n; i++) put(i, 0, A[i].w);
+            break;
+        case MFREE_P:
+            if ((st = copy_field_raw(c, c->rec.V, A))) return st;
+            if ((st = copy_field_raw(c, S.fc4, B))) return st;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            {
+                float c0 = std::sqrt(c->phys.rho0 != 0.f ? c->phys.K / c->phys.rho0 : 0.f);
+                for (int i = 0; i < n; i++) put(i, 0, B[i].w == 1.f ? 0.f : c0 * c0 * (A[i].w - c->phys.rho0));
+            }
+            break;
+        case MFREE_S:
+        case MFREE_S_T: {
+            if ((st = copy_field_raw(c, f == MFREE_S ? S.sa4 : S.dsa4, A))) return st;
+            if ((st = copy_field_raw(c, f == MFREE_S ? S.sb4 : S.dsb4, B))) return st;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            for (int i = 0; i < n; i++) {
+                float s6[6] = {A[i].x, A[i].y, A[i].z, A[i].w, B[i].x, B[i].y};
+                sym_to_9(s6, &tmp[size_t(i) * 9]);
+            }
+            break;
+        }
+        case MFREE_R:
+            if ((st = copy_field_raw(c, c->rec.R, A))) return st;
+            if ((st = copy_field_raw(c, c->rec.C, B))) return st;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            for (int i = 0; i < n; i++) {
+                float s6[6] = {A[i].x, A[i].y, A[i].z, A[i].w, B[i].x, B[i].y};
+                sym_to_9(s6, &tmp[size_t(i) * 9]);
+            }
+            break;
+        case MFREE_FC:
+        case MFREE_FT:
+        case MFREE_POS_T:
+        case MFREE_VEL_T: {
+            const float4 *src = f == MFREE_FC ? S.fc4 : f == MFREE_FT ? S.ft4 : f == MFREE_POS_T ? S.da4 : S.dv4;
+            if ((st = copy_field_raw(c, src, A))) return st;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            for (int i = 0; i < n; i++) { put(i, 0, A[i].x); put(i, 1, A[i].y); put(i, 2, A[i].z); }
+            break;
+        }
+        case MFREE_NRM:
+        case MFREE_POS_HALF: {
+            if (!c->opt.diagnostics) return fail(MFREE_ERR_ARG, "field kept only with options.diagnostics = 1");
+            if ((st = copy_field_raw(c, f == MFREE_NRM ? c->scr.nrm : c->scr.pos_half, A))) return st;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            for (int i = 0; i < n; i++) {
+                put(i, 0, A[i].x); put(i, 1, A[i].y); put(i, 2, A[i].z);
+                if (w == 4) put(i, 3, 0.f);
+            }
+            break;
+        }
+        case MFREE_FIXED:
+        case MFREE_EPS_PL_DOT:
+            if ((st = copy_field_raw(c, S.dsb4, A))) return st;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            for (int i = 0; i < n; i++) put(i, 0, f == MFREE_FIXED ? A[i].w : A[i].z);
+            break;
+        case MFREE_BLANKED:
+            if ((st = copy_field_raw(c, S.ft4, A))) return st;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            for (int i = 0; i < n; i++) put(i, 0, A[i].w);
+            break;
+        case MFREE_TOOL_PARTICLE:
+            if ((st = copy_field_raw(c, S.fc4, A))) return st;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            for (int i = 0; i < n; i++) put(i, 0, A[i].w);
+            break;
+        case MFREE_EPS_PL:
+        case MFREE_T:
+            if ((st = copy_field_raw(c, S.sb4, A))) return st;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            for (int i = 0; i < n; i++) put(i, 0, f == MFREE_T ? A[i].z : A[i].w);
+            break;
+        case MFREE_RHO_T:
+        case MFREE_T_T:
+            if ((st = copy_field_raw(c, f == MFREE_RHO_T ? S.da4 : S.dv4, A))) return st;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            for (int i = 0; i < n; i++) put(i, 0, A[i].w);
+            break;
+        case MFREE_NUM_NBH:
+            if (!c->opt.diagnostics) return fail(MFREE_ERR_ARG, "field kept only with options.diagnostics = 1");
+            return ints(c->scr.nnb, false);
+        case MFREE_IDX:
+            return ints(c->scr.perm, false);
+        case MFREE_HASH:
+            return ints((const int *)c->scr.key_sorted, true);
+        case MFREE_ID: {
+            if ((st = copy_field_raw(c, S.bc4, A))) return st;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            for (int i = 0; i < n; i++) {
+                int id;
+                std::memcpy(&id, &A[i].w, 4);
+                if (fo) std::memcpy(&fo[i], &id, 4);
+                if (dout) dout[i] = double(id);
+            }
+            return MFREE_OK;
+        }
+        default:
+            return fail(MFREE_ERR_ARG, "unknown field");
+    }
+    if (fo) std::memcpy(fo, tmp.data(), sizeof(float) * tmp.size());
+    if (dout)
+        for (size_t k = 0; k < tmp.size(); k++) dout[k] = double(tmp[k]);
+    return MFREE_OK;
+}
+
+}  // namespace
+
+int mfree_get_field(mfree_ctx *c, int f, void *out) {
+    if (!c || !out) return fail(MFREE_ERR_ARG, "null argument");
+    return get_field_impl(c, f, (float *)out, nullptr);
+}
+int mfree_get_field_f64(mfree_ctx *c, int f, double *out) {
+    if (!c || !out) return fail(MFREE_ERR_ARG, "null argument");
+    return get_field_impl(c, f, nullptr, out);
+}
+
+int mfree_set_field(mfree_ctx *c, int f, const void *in) {
+    if (!c || !in) return fail(MFREE_ERR_ARG, "null argument");
+    const int n = c->n_init;
+    const State &S = c->st[c->cur];
+    const float *v = (const float *)in;
+    std::vector<float4> A, B;
+    int st;
+    auto rw = [&](float4 *dst, std::vector<float4> &buf, auto fn) -> int {
+        if ((st = copy_field_raw(c, dst, buf))) return st;
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        for (int i = 0; i < n; i++) fn(i, buf[i]);
+        CUDA_TRY(cudaMemcpyAsync(dst, buf.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, c->stream));
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        return MFREE_OK;
+    };
+    invalidate_graphs(c);
+    switch (f) {
+        case MFREE_POS: return rw(S.pos4, A, [&](int i, float4 &x) { x.x = v[4*i]; x.y = v[4*i+1]; x.z = v[4*i+2]; });
+        case MFREE_VEL: return rw(S.vel4, A, [&](int i, float4 &x) { x.x = v[4*i]; x.y = v[4*i+1]; x.z = v[4*i+2]; });
+        case MFREE_VEL_BC: return rw(S.bc4, A, [&](int i, float4 &x) { x.x = v[4*i]; x.y = v[4*i+1]; x.z = v[4*i+2]; });
+        case MFREE_H: return rw(S.pos4, A, [&](int i, float4 &x) { x.w = v[i]; });
+        case MFREE_RHO: return rw(S.vel4, A, [&](int i, float4 &x) { x.w = v[i]; });
+        case MFREE_S:
+            if ((st = rw(S.sa4, A, [&](int i, float4 &x) { x.x = v[9*i]; x.y = v[9*i+4]; x.z = v[9*i+8]; x.w = v[9*i+1]; }))) return st;
+            return rw(S.sb4, B, [&](int i, float4 &x) { x.x = v[9*i+2]; x.y = v[9*i+5]; });
+        case MFREE_S_T:
+            if ((st = rw(S.dsa4, A, [&](int i, float4 &x) { x.x = v[9*i]; x.y = v[9*i+4]; x.z = v[9*i+8]; x.w = v[9*i+1]; }))) return st;
+            return rw(S.dsb4, B, [&](int i, float4 &x) { x.x = v[9*i+2]; x.y = v[9*i+5]; });
+        case MFREE_FC: return rw(S.fc4, A, [&](int i, float4 &x) { x.x = v[3*i]; x.y = v[3*i+1]; x.z = v[3*i+2]; });
+        case MFREE_FT: return rw(S.ft4, A, [&](int i, float4 &x) { x.x = v[3*i]; x.y = v[3*i+1]; x.z = v[3*i+2]; });
+        case MFREE_POS_T: return rw(S.da4, A, [&](int i, float4 &x) { x.x = v[3*i]; x.y = v[3*i+1]; x.z = v[3*i+2]; });
+        case MFREE_VEL_T: return rw(S.dv4, A, [&](int i, float4 &x) { x.x = v[3*i]; x.y = v[3*i+1]; x.z = v[3*i+2]; });
+        case MFREE_RHO_T: return rw(S.da4, A, [&](int i, float4 &x) { x.w = v[i]; });
+        case MFREE_T_T: return rw(S.dv4, A, [&](int i, float4 &x) { x.w = v[i]; });
+        case MFREE_FIXED: return rw(S.dsb4, A, [&](int i, float4 &x) { x.w = v[i]; });
+        case MFREE_EPS_PL_DOT: return rw(S.dsb4, A, [&](int i, float4 &x) { x.z = v[i]; });
+        case MFREE_BLANKED: return rw(S.ft4, A, [&](int i, float4 &x) { x.w = v[i]; });
+        case MFREE_TOOL_PARTICLE: return rw(S.fc4, A, [&](int i, float4 &x) { x.w = v[i]; });
+        case MFREE_EPS_PL: return rw(S.sb4, A, [&](int i, float4 &x) { x.w = v[i]; });
+        case MFREE_T: return rw(S.sb4, A, [&](int i, float4 &x) { x.z = v[i]; });
+        default: return fail(MFREE_ERR_ARG, "field cannot be set");
+    }
+}
+
+int mfree_get_cells(mfree_ctx *c, int *cs, int *ce) {
+    if (!c || !cs || !ce) return fail(MFREE_ERR_ARG, "null argument");
+    if (!c->grid_set || c->scratch_allocs.empty()) return fail(MFREE_ERR_ARG, "no step has run");
+    std::vector<int> first(c->num_cell + 1);
+    CUDA_TRY(cudaMemcpyAsync(first.data(), c->scr.first, sizeof(int) * (c->num_cell + 1), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (long k = 0; k < c->num_cell; k++) {
+        if (first[k + 1] > first[k]) {
+            cs[k] = first[k];
+            ce[k] = first[k + 1];
+        } else {
+            cs[k] = -1;
+            ce[k] = -1;
+        }
+    }
+    return MFREE_OK;
+}
+
+int mfree_get_grid(const mfree_ctx *c, long *nx, long *ny, long *nz, float *bbmin3, float *dx) {
+    if (!c || !c->grid_set) return fail(MFREE_ERR_ARG, "grid not set");
+    if (nx) *nx = c->nx;
+    if (ny) *ny = c->ny;
+    if (nz) *nz = c->nz;
+    if (bbmin3)
+        for (int d = 0; d < 3; d++) bbmin3[d] = c->g_bbmin[d];
+    if (dx) *dx = c->g_dx;
+    return MFREE_OK;
+}
+
+void mfree_free(void *p) { free(p); }
+
+}  // extern "C"

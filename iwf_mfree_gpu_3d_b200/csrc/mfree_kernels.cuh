@@ -1,0 +1,88 @@
+// mfree_kernels.cuh -- kernel declarations and helpers shared by the step's
+// translation units.
+#pragma once
+
+#include "mfree_device.cuh"
+
+namespace mfree {
+
+constexpr int HASH_BLOCK = 256;
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+constexpr int INTERACT_WARPS = 4;  // warps per block of the pair kernel
+constexpr int QCAP = 128;          // in-support queue per particle before the rescan path
+constexpr int NRES = 20;           // reduced accumulators per particle
+
+// half-step state x + dt/2 * xdot of the predictor (leap_frog.cu:42-70); the
+// pair kernel's epilogue recomputes it with the same expressions
+struct HalfStep {
+    float x, y, z, vx, vy, vz, rho, T;
+    float S[6];  // xx yy zz xy xz yz
+};
+
+template <bool PREC>
+__device__ __forceinline__ HalfStep half_step(float h2, float4 pos, float4 vel, float4 sa, float4 sb, float4 da,
+                                              float4 dv, float4 dsa, float4 dsb, float4 lo, float4 lob) {
+    HalfStep o;
+    if (PREC) {
+        o.x = pos.x + fmaf(h2, da.x, lo.x);
+        o.y = pos.y + fmaf(h2, da.y, lo.y);
+        o.z = pos.z + fmaf(h2, da.z, lo.z);
+        o.vx = vel.x + fmaf(h2, dv.x, lo.w);
+        o.vy = vel.y + fmaf(h2, dv.y, lob.x);
+        o.vz = vel.z + fmaf(h2, dv.z, lob.y);
+    } else {
+        o.x = fmaf(h2, da.x, pos.x);
+        o.y = fmaf(h2, da.y, pos.y);
+        o.z = fmaf(h2, da.z, pos.z);
+        o.vx = fmaf(h2, dv.x, vel.x);
+        o.vy = fmaf(h2, dv.y, vel.y);
+        o.vz = fmaf(h2, dv.z, vel.z);
+    }
+    o.rho = fmaf(h2, da.w, vel.w);
+    o.T = fmaf(h2, dv.w, sb.z);
+    o.S[0] = fmaf(h2, dsa.x, sa.x);
+    o.S[1] = fmaf(h2, dsa.y, sa.y);
+    o.S[2] = fmaf(h2, dsa.z, sa.z);
+    o.S[3] = fmaf(h2, dsa.w, sa.w);
+    o.S[4] = fmaf(h2, dsb.x, sb.x);
+    o.S[5] = fmaf(h2, dsb.y, sb.y);
+    return o;
+}
+
+// particle inside the box of tool k at this step (the contact kernels' early
+// reject, tool_3d_gpu.cu:607-614), for a tool that is set up and alive
+__device__ __forceinline__ bool in_tool_box(const StepArgs &a, int k, float x, float y, float z) {
+    const ToolDev &T = a.tools[k];
+    if (T.num_tris == 0) return false;
+    const DevClock *c = a.clk;
+    if (c->t < T.birth || c->t > T.death) return false;
+    const ToolClock &b = c->tool[k];
+    return x > b.bbmin[0] && x < b.bbmax[0] && y > b.bbmin[1] && y < b.bbmax[1] && z > b.bbmin[2] && z < b.bbmax[2];
+}
+__device__ __forceinline__ bool contact_candidate(const StepArgs &a, float x, float y, float z) {
+    bool in = false;
+    for (int k = 0; k < a.p.num_tools; k++) in |= in_tool_box(a, k, x, y, z);
+    return in;
+}
+
+__global__ void k_clock(StepArgs a, int record_mode);
+__global__ void k_hash(StepArgs a);
+__global__ void k_scan_reduce(StepArgs a);
+__global__ void k_scan_top(StepArgs a, int num_tiles, int num_hash_blocks);
+__global__ void k_scan_down(StepArgs a);
+__global__ void k_scatter(StepArgs a);
+__global__ void k_cell_fixup(StepArgs a);
+cudaError_t launch_gather_predict(const StepArgs &a, int blocks, cudaStream_t s);
+__global__ void k_finalize(StepArgs a);
+__global__ void k_force_final(StepArgs a, int num_blocks, float *out);
+
+// launches the pair kernel for the configured variant (mfree_interact.cu)
+cudaError_t launch_interact(const StepArgs &a, int lanes_per_particle, int grid, cudaStream_t s);
+int interact_grid_size(int lanes_per_particle, int n_init, int num_sms);
+
+// sustained FP32 FMA throughput of the current device in TFLOP/s (mfree_probe.cu)
+double fp32_peak_probe(int num_sms);
+
+}  // namespace mfree

@@ -1,0 +1,289 @@
+// mfree_sort.cu -- start of the step: clock, blanking + cell hash, stable
+// counting sort by cell, and the gather that fuses the reorder with the
+// predictor, the equation of state and the artificial stress.
+//
+// Reference path replaced (src/leap_frog.cu:133-151):
+//   blanking::update + do_blanking          actions_gpu.cu:489-531, blanking.cpp:43-51
+//   grid_base::update_geometry (locked)     grid_gpu_base.cu:166-183
+//   compute_hashes                          grid_gpu_base.cu:41-63
+//   adapt_particle_number (thrust::count)   grid_gpu_base.cu:141-164
+//   do_sort: sequence + stable sort_by_key, cell range build, reorder_data
+//                                           grid_gpu_green.cu:24-125,265-297
+//   init, predict                           leap_frog.cu:30-70
+//   do_material_eos, do_corrector_artificial_stress  actions_gpu.cu:40-132
+//
+// The sort is a stable counting sort: an atomic histogram of cell ids, an
+// exclusive scan (which is also the cell-range table the pair loop reads),
+// an atomic scatter and a per-cell fix-up that orders each cell's entries by
+// their previous index.  The result equals thrust's stable sort_by_key of
+// (cell id, 0..n-1): cells ascending, previous order inside a cell, blanked
+// particles (cell id INT_MAX in the reference) last in previous order.
+// N stays on the device: no host round trip per step.
+#include "mfree_kernels.cuh"
+
+namespace mfree {
+
+// ----------------------------------------------------------------- clock --
+// record_mode: 0 no, 1 yes, 2 every Params::record_every steps
+__global__ void k_clock(StepArgs a, int record_mode) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    DevClock *c = a.clk;
+    const Params &P = a.p;
+    if (c->pending) c->t = c->t + P.dt;  // main(): global_time_current += dt after each iteration
+    c->pending = 1;
+    const float t = c->t;
+    c->record = record_mode == 1 ? 1
+                : record_mode == 2 ? (P.record_every > 0 && (c->step_index % P.record_every) == 0)
+                                   : 0;
+    c->step_index++;
+    if (P.blank_on)
+        for (int d = 0; d < 3; d++) {
+            c->blank_min[d] = P.blank_min0[d] + t * P.blank_vel[d];
+            c->blank_max[d] = P.blank_max0[d] + t * P.blank_vel[d];
+        }
+    if (P.grid_moving)
+        for (int d = 0; d < 3; d++) c->grid_min[d] = P.grid_min0[d] + t * P.grid_vel[d];
+    for (int k = 0; k < P.num_tools; k++) {
+        if (a.tools[k].num_tris == 0) continue;  // update_tool returns early without boxed triangles
+        for (int d = 0; d < 3; d++) {
+            c->tool[k].bbmin[d] += P.dt * a.tools[k].vel[d];
+            c->tool[k].bbmax[d] += P.dt * a.tools[k].vel[d];
+        }
+    }
+}
+
+// ------------------------------------------------- blanking + cell hash --
+__global__ void __launch_bounds__(HASH_BLOCK) k_hash(StepArgs a) {
+    const Params &P = a.p;
+    const int i = blockIdx.x * HASH_BLOCK + threadIdx.x;
+    int blank = 0;
+    if (i < P.n_init) {
+        float4 p = a.a.pos4[i];
+        float4 ft = a.a.ft4[i];
+        float blanked = ft.w;
+        if (P.blank_on) {
+            float4 v = a.a.vel4[i];
+            const DevClock *c = a.clk;
+            bool fast = __fadd_rn(__fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y)), __fmul_rn(v.z, v.z)) >= P.vmax2;
+            bool in = p.x >= c->blank_min[0] && p.x <= c->blank_max[0] && p.y >= c->blank_min[1] &&
+                      p.y <= c->blank_max[1] && p.z >= c->blank_min[2] && p.z <= c->blank_max[2];
+            if (fast || !in) {
+                blanked = 1.f;
+            } else {
+                float4 da = a.a.da4[i], dv = a.a.dv4[i], dsa = a.a.dsa4[i], dsb = a.a.dsb4[i];
+                bool bad = nan_or_inf(da.x) || nan_or_inf(da.y) || nan_or_inf(da.z) || nan_or_inf(dv.x) ||
+                           nan_or_inf(dv.y) || nan_or_inf(dv.z) || nan_or_inf(dsa.x) || nan_or_inf(dsa.y) ||
+                           nan_or_inf(dsa.z) || nan_or_inf(dsa.w) || nan_or_inf(dsb.y) || nan_or_inf(dsb.x) ||
+                           nan_or_inf(da.w) || nan_or_inf(dv.w);
+                if (!bad) blanked = 0.f;
+                else if (blanked == 1.f) atomicAdd(&a.clk->nan_blanked, 1ull);
+            }
+        }
+        unsigned key = unsigned(P.num_cell);
+        if (blanked != 1.f) {
+            const float *gmin = P.grid_moving ? a.clk->grid_min : P.grid_min0;
+            int ix = int(__fdiv_rn(__fsub_rn(p.x, gmin[0]), P.gdx));
+            int iy = int(__fdiv_rn(__fsub_rn(p.y, gmin[1]), P.gdx));
+            int iz = int(__fdiv_rn(__fsub_rn(p.z, gmin[2]), P.gdx));
+            if (ix >= 0 && ix < P.gnx && iy >= 0 && iy < P.gny && iz >= 0 && iz < P.gnz) {
+                key = unsigned((ix * P.gny + iy) * P.gnz + iz);
+            } else {
+                blanked = 1.f;  // outside the cell grid but not blanked: taken out (counted)
+                atomicAdd(&a.clk->out_of_grid, 1ull);
+            }
+        }
+        if (blanked != ft.w) {
+            ft.w = blanked;
+            a.a.ft4[i] = ft;
+        }
+        a.s.key[i] = key;
+        if (key < unsigned(P.num_cell)) atomicAdd(&a.s.count[key], 1);
+        else blank = 1;
+    }
+    int nb = __syncthreads_count(blank);
+    if (threadIdx.x == 0) a.s.blank_block[blockIdx.x] = nb;
+}
+
+// ------------------------------------------------------------- the scan --
+// exclusive scan of count[0..num_cell) into first[0..num_cell]; first[num_cell] = N
+__device__ __forceinline__ int block_exclusive_scan(int v, int *warp_sums, int &total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < (blockDim.x >> 5) ? warp_sums[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        warp_sums[lane] = w;  // inclusive
+    }
+    __syncthreads();
+    int pre = warp > 0 ? warp_sums[warp - 1] : 0;
+    total = warp_sums[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return pre + x - v;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(StepArgs a) {
+    __shared__ int ws[32];
+    const int nc = a.p.num_cell;
+    const int base = blockIdx.x * SCAN_TILE;
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        int c = base + threadIdx.x + k * SCAN_THREADS;
+        if (c < nc) s += a.s.count[c];
+    }
+    int total;
+    block_exclusive_scan(s, ws, total);
+    if (threadIdx.x == 0) a.s.tile_sum[blockIdx.x] = total;
+}
+
+// one block: exclusive scans of the tile sums and of the blanked-per-block counts
+__global__ void __launch_bounds__(1024) k_scan_top(StepArgs a, int num_tiles, int num_hash_blocks) {
+    __shared__ int ws[32];
+    __shared__ int carry;
+    for (int pass = 0; pass < 2; pass++) {
+        int *arr = pass == 0 ? a.s.tile_sum : a.s.blank_block;
+        const int n = pass == 0 ? num_tiles : num_hash_blocks;
+        if (threadIdx.x == 0) carry = 0;
+        __syncthreads();
+        for (int b0 = 0; b0 < n; b0 += 1024) {
+            int idx = b0 + threadIdx.x;
+            int v = idx < n ? arr[idx] : 0;
+            int total;
+            int ex = block_exclusive_scan(v, ws, total);
+            int c0 = carry;
+            if (idx < n) arr[idx] = c0 + ex;
+            __syncthreads();
+            if (threadIdx.x == 0) carry = c0 + total;
+            __syncthreads();
+        }
+        if (pass == 0 && threadIdx.x == 0) a.clk->n_active = carry;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(StepArgs a) {
+    __shared__ int ws[32];
+    const int nc = a.p.num_cell;
+    const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    int v[SCAN_ITEMS];
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        int c = base + k;
+        v[k] = c < nc ? a.s.count[c] : 0;
+        s += v[k];
+    }
+    int total;
+    int ex = block_exclusive_scan(s, ws, total) + a.s.tile_sum[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        int c = base + k;
+        if (c <= nc) a.s.first[c] = ex;  // first[nc] = N
+        ex += v[k];
+    }
+}
+
+// ---------------------------------------------------------- the scatter --
+__global__ void __launch_bounds__(HASH_BLOCK) k_scatter(StepArgs a) {
+    __shared__ int ws[32];
+    const Params &P = a.p;
+    const int i = blockIdx.x * HASH_BLOCK + threadIdx.x;
+    const int N = a.clk->n_active;
+    unsigned key = i < P.n_init ? a.s.key[i] : 0u;
+    int blank = (i < P.n_init && key >= unsigned(P.num_cell)) ? 1 : 0;
+    int total;
+    int rank = block_exclusive_scan(blank, ws, total);
+    if (i >= P.n_init) return;
+    if (!blank) {
+        int old = atomicSub(&a.s.count[key], 1);  // leaves count[] zero for the next step
+        a.s.perm[a.s.first[key] + old - 1] = i;
+    } else {
+        a.s.perm[N + a.s.blank_block[blockIdx.x] + rank] = i;
+    }
+}
+
+// order each cell's entries by previous index (stable within the cell)
+__global__ void k_cell_fixup(StepArgs a) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.p.num_cell) return;
+    const int s = a.s.first[c], e = a.s.first[c + 1];
+    if (e - s < 2) return;
+    int *p = a.s.perm;
+    for (int k = s + 1; k < e; k++) {
+        int v = p[k];
+        int m = k - 1;
+        while (m >= s && p[m] > v) {
+            p[m + 1] = p[m];
+            m--;
+        }
+        p[m + 1] = v;
+    }
+}
+
+// --------------------------------------------- gather + predictor + EOS --
+template <bool PREC>
+__global__ void __launch_bounds__(256) k_gather_predict(StepArgs a) {
+    const Params &P = a.p;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n_init) return;
+    const int N = a.clk->n_active;
+    int src = a.s.perm[i];
+    if (src < 0 || src >= P.n_init) {  // cannot happen for a consistent sort; never read out of bounds
+        atomicAdd(&a.clk->out_of_grid, 1ull << 32);
+        src = i;
+    }
+    const State &A = a.a, &B = a.b;
+    float4 pos = A.pos4[src], vel = A.vel4[src], sa = A.sa4[src], sb = A.sb4[src];
+    float4 da = A.da4[src], dv = A.dv4[src], dsa = A.dsa4[src], dsb = A.dsb4[src];
+    float4 fc = A.fc4[src], ft = A.ft4[src], bc = A.bc4[src];
+    B.pos4[i] = pos; B.vel4[i] = vel; B.sa4[i] = sa; B.sb4[i] = sb;
+    B.da4[i] = da; B.dv4[i] = dv; B.dsa4[i] = dsa; B.dsb4[i] = dsb;
+    B.fc4[i] = fc; B.ft4[i] = ft; B.bc4[i] = bc;
+    float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), lob = lo;
+    if (PREC) {
+        lo = A.lo4[src];
+        lob = A.lo4b[src];
+        B.lo4[i] = lo;
+        B.lo4b[i] = lob;
+    }
+    a.s.key_sorted[i] = a.s.key[src];
+    if (i >= N) return;  // blanked: frozen
+    const float h2 = 0.5f * P.dt;
+    HalfStep hs = half_step<PREC>(h2, pos, vel, sa, sb, da, dv, dsa, dsb, lo, lob);
+    const bool tool = fc.w == 1.f;
+    float prs = 0.f;
+    float Rr[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (!tool) {
+        prs = P.c0sq * (hs.rho - P.rho0);
+        if (P.stresseps != 0.f)
+            artificial_stress(hs.S[0], hs.S[1], hs.S[2], hs.S[3], hs.S[4], hs.S[5], prs, hs.rho, P.stresseps, Rr);
+    }
+    const float ir2 = 1.0f / (hs.rho * hs.rho);
+    Records r = a.r;
+    r.P[i] = make_float4(hs.x, hs.y, hs.z, fc.w);  // raw tool_particle value
+    r.V[i] = make_float4(hs.vx, hs.vy, hs.vz, hs.rho);
+    r.A[i] = make_float4((hs.S[0] - prs) * ir2, (hs.S[1] - prs) * ir2, (hs.S[2] - prs) * ir2, hs.S[3] * ir2);
+    r.B[i] = make_float4(hs.S[4] * ir2, hs.S[5] * ir2, sqrtf(P.K / hs.rho), pos.w);
+    r.R[i] = make_float4(Rr[0], Rr[1], Rr[2], Rr[3]);
+    r.C[i] = make_float4(Rr[4], Rr[5], hs.T, P.mass / hs.rho);
+    if (P.diagnostics) a.s.pos_half[i] = make_float4(hs.x, hs.y, hs.z, 0.f);
+}
+
+cudaError_t launch_gather_predict(const StepArgs &a, int blocks, cudaStream_t s) {
+    if (a.p.precision) k_gather_predict<true><<<blocks, 256, 0, s>>>(a);
+    else k_gather_predict<false><<<blocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace mfree

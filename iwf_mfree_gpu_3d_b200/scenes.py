@@ -1,0 +1,302 @@
+"""Cutting scenes in the reference's cm-g-us unit system.
+
+The reference builds its scenes in C++ setup functions (for example
+setup_single_grain_1tool, src/Benchmarks/benchmarks_single_grain.cu:674-876):
+an x-major particle lattice with z = -k*dx, steel/titanium constants in
+cm-g-us, a rigid triangulated tool, a locked cell grid and a blanking box of
+the lattice and tool padded by 15*dx, dt = 0.5*CFL*h/(sqrt(v_tool) + c0).
+
+This module builds the same kind of scene with seeded, deterministic inputs:
+
+  * ``orthogonal_cutting(nx, ny, nz, ...)``: a steel block cut by a 12-triangle
+    wedge (0 deg rake, 7 deg clearance) at the +x face -- the 8k and 1M
+    workloads;
+  * ``single_grain(...)``: a block cut by a truncated icosphere grain.
+
+The scene is plain numpy data; the CUDA path (``api.Simulation``) and the CPU
+oracle consume the same arrays.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import List, Optional
+
+import numpy as np
+
+# ---------------------------------------------------------------- seeding --
+
+_U64 = np.uint64
+
+
+def splitmix64(seed: int, n: int) -> np.ndarray:
+    """n outputs of the SplitMix64 generator (Steele, Lea, Flood 2014)."""
+    with np.errstate(over="ignore"):
+        k = np.arange(1, n + 1, dtype=np.uint64)
+        x = _U64(seed & 0xFFFFFFFFFFFFFFFF) + k * _U64(0x9E3779B97F4A7C15)
+        z = x
+        z = (z ^ (z >> _U64(30))) * _U64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> _U64(27))) * _U64(0x94D049BB133111EB)
+        return z ^ (z >> _U64(31))
+
+
+def uniform_pm1(seed: int, n: int) -> np.ndarray:
+    """n doubles uniform in [-1, 1) from SplitMix64."""
+    u = (splitmix64(seed, n) >> _U64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    return 2.0 * u - 1.0
+
+
+# ------------------------------------------------------------------ scene --
+
+@dataclasses.dataclass
+class Tool:
+    verts: np.ndarray          # (nv, 3) float32
+    tris: np.ndarray           # (nt, 3) int32, closed manifold
+    vel: np.ndarray            # (3,) float32, cm/us
+    contact_alpha: float = 0.1  # tool_3d_gpu.h:131-134 default
+    mu: float = 0.35
+    algorithm: int = 0         # 0 = spatial hashing (safe), 1 = exhaustive
+
+
+@dataclasses.dataclass
+class Scene:
+    name: str
+    pos: np.ndarray            # (n, 4) float32
+    vel: np.ndarray            # (n, 4) float32
+    rho: np.ndarray            # (n,) float32
+    T: np.ndarray
+    h: np.ndarray
+    fixed: np.ndarray
+    tool_p: np.ndarray
+    phys: dict
+    corr: dict
+    joco: Optional[dict]
+    trml_wp: dict
+    trml_tool: dict
+    options: dict
+    grid_bbmin: np.ndarray
+    grid_bbmax: np.ndarray
+    grid_h: float
+    blank_bbmin: np.ndarray
+    blank_bbmax: np.ndarray
+    blank_vmax: float
+    dt: float
+    tools: List[Tool]
+
+    @property
+    def n(self) -> int:
+        return int(self.pos.shape[0])
+
+
+# steel in cm-g-us (E, K, G in Mbar; 1 Mbar = 1e11 Pa)
+STEEL = dict(rho0=7.83, E=2.0, nu=0.29)
+STEEL_JC = dict(A=7.92e-3, B=5.10e-3, C=0.014, n=0.26, m=1.03, Tmelt=1793.0, Tref=300.0,
+                eps_dot_ref=1e-6, clamp_temp=1.0)
+
+
+def kernel_value(r: float, h: float) -> float:
+    """cubic_spline value W(r, h) (src/kernels.cuh:26-69), in double."""
+    q = r / h
+    fac = 1.0 / math.pi / h ** 3
+    if q > 1.0:
+        return 0.25 * (2.0 - q) ** 3 * fac
+    return (1.0 - 1.5 * q * q * (1.0 - 0.5 * q)) * fac
+
+
+def material(dx: float, hdx: float = 1.3, rho0=STEEL["rho0"], E=STEEL["E"], nu=STEEL["nu"],
+             art_stress: float = 0.3):
+    G = E / (2.0 * (1.0 + nu))
+    K = 2.0 * G * (1.0 + nu) / (3.0 * (1.0 - 2.0 * nu))
+    phys = dict(E=E, nu=nu, rho0=rho0, K=K, G=G, mass=dx ** 3 * rho0)
+    corr = dict(wdeltap=kernel_value(dx, hdx * dx), stresseps=art_stress, xspheps=0.5,
+                alpha=1.0, beta=1.0, eta=0.1)
+    return phys, corr
+
+
+def steel_thermal(rho0: float = STEEL["rho0"]):
+    k = 50.0 * 1e-13        # W/(m K) -> cm-g-us
+    cp = 477.0 * 1e-8       # J/(kg K) -> cm-g-us
+    return dict(cp=cp, tq=0.9, k=k, alpha=k / (rho0 * cp), T_init=300.0, eta=0.9)
+
+
+def time_step(h: float, v_tool: float, K: float, rho0: float, cfl: float = 0.3) -> float:
+    """dt = 0.5 * CFL * h / (sqrt(v_tool) + c0) (benchmarks_single_grain.cu:849-851)."""
+    c0 = math.sqrt(K / rho0)
+    return float(np.float32(0.5 * cfl * h / (math.sqrt(v_tool) + c0)))
+
+
+def wedge_tool(x_edge: float, z_edge: float, y0: float, y1: float, dx: float,
+               rake_deg: float = 0.0, clearance_deg: float = 7.0,
+               height: float = 10.0, length: float = 10.0):
+    """Closed 12-triangle wedge (a hexahedron) cutting towards -x.
+
+    Cross-section in x-z: cutting edge E=(x_edge, z_edge); the rake face rises
+    from E to z_edge+height*dx, leaning back by the rake angle; the clearance face
+    leaves E towards +x at the clearance angle; the tool is extruded over
+    y0..y1."""
+    H = height * dx
+    L = length * dx
+    zt = z_edge + H
+    xr = x_edge + H * math.tan(math.radians(rake_deg))
+    xc = x_edge + L
+    zc = z_edge + L * math.tan(math.radians(clearance_deg))
+    sec = [(x_edge, z_edge), (xr, zt), (xc + max(0.0, xr - x_edge), zt), (xc, zc)]
+    v = []
+    for y in (y0, y1):
+        for (x, z) in sec:
+            v.append((x, y, z))
+    verts = np.array(v, dtype=np.float32)
+    # quads of the hexahedron (vertices 0-3 at y0, 4-7 at y1)
+    quads = [(0, 1, 2, 3), (4, 7, 6, 5), (0, 4, 5, 1), (1, 5, 6, 2), (2, 6, 7, 3), (3, 7, 4, 0)]
+    tris = []
+    for (a, b, c, d) in quads:
+        tris.append((a, b, c))
+        tris.append((a, c, d))
+    return verts, np.array(tris, dtype=np.int32)
+
+
+def lattice(nx: int, ny: int, nz: int, dx: float, seed: int = 0, jitter: float = 0.01):
+    """x-major lattice (for i, for j, for k) with z = -k*dx and y centred, as
+    benchmarks_single_grain.cu:720-737, plus a uniform +-jitter*dx per
+    coordinate from SplitMix64."""
+    ly = ny * dx
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    p = np.stack([i.ravel() * dx, j.ravel() * dx - ly / 2.0, -k.ravel() * dx], axis=1)
+    n = p.shape[0]
+    if jitter:
+        p = p + jitter * dx * uniform_pm1(seed, 3 * n).reshape(n, 3)
+    pos = np.zeros((n, 4), dtype=np.float32)
+    pos[:, :3] = p.astype(np.float32)
+    return pos
+
+
+def orthogonal_cutting(nx: int = 40, ny: int = 20, nz: int = 10, dx: float = 1.0e-3,
+                       v_tool: float = 1.0e-3, depth: float = 5.0, engage: float = 0.05,
+                       seed: int = 0, cspm: bool = False, conduction: int = 1,
+                       art_stress: float = 0.3, precision: int = 0, hdx: float = 1.3,
+                       plastic: bool = True, algorithm: int = 0,
+                       rake_deg: float = 0.0, jc_scale=(1.0, 1.0, 1.0),
+                       name: Optional[str] = None) -> Scene:
+    """Orthogonal cutting of a steel block by a rigid wedge.
+
+    nx*ny*nz particles on a jittered lattice of spacing dx (cm); the wedge's
+    cutting edge sits depth*dx below the top surface and overlaps the +x face
+    by engage*dx (at 10 m/s the tool moves only ~4e-4 dx per step, so it has to
+    start engaged); it moves towards -x at v_tool cm/us.  The bottom layer is
+    fixed.  conduction: 0 none, 1 Brookshaw, 2 PSE."""
+    h = hdx * dx
+    pos = lattice(nx, ny, nz, dx, seed=seed)
+    n = pos.shape[0]
+    phys, corr = material(dx, hdx, art_stress=art_stress)
+    joco = dict(STEEL_JC)
+    joco["A"] *= jc_scale[0]
+    joco["B"] *= jc_scale[1]
+    joco["n"] *= jc_scale[2]
+    twp = steel_thermal(phys["rho0"])
+    ttool = dict(cp=0.0, tq=0.0, k=0.0, alpha=0.0, T_init=0.0, eta=0.0)
+    lz = (nz - 1) * dx
+    lx = (nx - 1) * dx
+    ly = ny * dx
+    fixed = (pos[:, 2] < -lz + dx / 2.0).astype(np.float32)
+    verts, tris = wedge_tool(x_edge=lx - engage * dx, z_edge=-depth * dx,
+                             y0=-ly / 2.0 - 2.0 * dx, y1=ly / 2.0 + 2.0 * dx, dx=dx,
+                             rake_deg=rake_deg)
+    tool = Tool(verts=verts, tris=tris, vel=np.array([-v_tool, 0.0, 0.0], np.float32),
+                mu=0.35, contact_alpha=0.1, algorithm=algorithm)
+    pad = 15.0 * dx
+    lo = np.minimum(pos[:, :3].min(0), verts.min(0)) - pad
+    hi = np.maximum(pos[:, :3].max(0), verts.max(0)) + pad
+    dt = time_step(h, v_tool, phys["K"], phys["rho0"])
+    options = dict(cspm=int(cspm), conduction=int(conduction), precision=int(precision),
+                   max_secant_iter=100, lanes_per_particle=0, diagnostics=0, friction_tool_vel=0)
+    return Scene(
+        name=name or f"cut_{nx}x{ny}x{nz}",
+        pos=pos,
+        vel=np.zeros((n, 4), np.float32),
+        rho=np.full(n, phys["rho0"], np.float32),
+        T=np.full(n, twp["T_init"], np.float32),
+        h=np.full(n, h, np.float32),
+        fixed=fixed,
+        tool_p=np.zeros(n, np.float32),
+        phys=phys, corr=corr, joco=joco if plastic else None,
+        trml_wp=twp, trml_tool=ttool, options=options,
+        grid_bbmin=lo.astype(np.float32), grid_bbmax=hi.astype(np.float32), grid_h=float(np.float32(h)),
+        blank_bbmin=lo.astype(np.float32), blank_bbmax=hi.astype(np.float32), blank_vmax=4.0,
+        dt=dt, tools=[tool])
+
+
+def small_scene(**kw) -> Scene:
+    """40 x 20 x 10 = 8,000 particles, Brookshaw, no CSPM (the 8k workload)."""
+    return orthogonal_cutting(40, 20, 10, **kw)
+
+
+def million_scene(**kw) -> Scene:
+    """200 x 100 x 50 = 1,000,000 particles, CSPM + artificial stress + PSE."""
+    kw.setdefault("cspm", True)
+    kw.setdefault("conduction", 2)
+    return orthogonal_cutting(200, 100, 50, **kw)
+
+
+# ------------------------------------------------------------ icosphere --
+
+def icosphere(subdiv: int = 3, radius: float = 1.0):
+    """Icosphere of 20 * 4**subdiv triangles (vertices on the sphere)."""
+    t = (1.0 + math.sqrt(5.0)) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    v = [np.array(p, float) / np.linalg.norm(p) for p in v]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+         (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5),
+         (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdiv):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = v[a] + v[b]
+                v.append(m / np.linalg.norm(m))
+                cache[key] = len(v) - 1
+            return cache[key]
+
+        nf = []
+        for (a, b, c) in f:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        f = nf
+    return np.array(v) * radius, np.array(f, dtype=np.int32)
+
+
+def truncated_grain(radius: float, rake_deg: float = -10.0, cut: float = 0.5):
+    """Icosphere grain flattened by the rake plane: vertices beyond the plane
+    are projected onto it, which keeps the 1,280 triangles and the mesh closed.
+    The plane faces -x (the cutting direction), tilted by the rake angle."""
+    v, f = icosphere(3, radius)
+    a = math.radians(rake_deg)
+    n = np.array([-math.cos(a), 0.0, math.sin(a)])   # outward normal of the rake face
+    d = cut * radius
+    s = v @ n - d
+    v = v - np.maximum(s, 0.0)[:, None] * n[None, :]
+    return v, f
+
+
+def single_grain(nx: int = 400, ny: int = 160, nz: int = 64, dx: float = 1.0e-3, v_tool: float = 3.0e-3,
+                 depth: float = 8.0, seed: int = 0, precision: int = 1, engage: float = 0.05) -> Scene:
+    """Single-grain cutting: a 1,280-triangle truncated icosphere of radius
+    20*dx at 30 m/s, depth of cut 8*dx, Brookshaw conduction."""
+    sc = orthogonal_cutting(nx, ny, nz, dx=dx, v_tool=v_tool, depth=depth, seed=seed,
+                            precision=precision, name=f"grain_{nx}x{ny}x{nz}")
+    R = 20.0 * dx
+    v, f = truncated_grain(R)
+    lx = (nx - 1) * dx
+    # place the flattened face on the +x face, its lowest point depth*dx below the top
+    v = v.copy()
+    v[:, 0] += lx - engage * dx - v[:, 0].min()
+    v[:, 2] += -depth * dx - v[:, 2].min()
+    sc.tools = [Tool(verts=v.astype(np.float32), tris=f, vel=np.array([-v_tool, 0, 0], np.float32))]
+    pad = 15.0 * dx
+    lo = np.minimum(sc.pos[:, :3].min(0), v.min(0)) - pad
+    hi = np.maximum(sc.pos[:, :3].max(0), v.max(0)) + pad
+    sc.grid_bbmin = sc.blank_bbmin = lo.astype(np.float32)
+    sc.grid_bbmax = sc.blank_bbmax = hi.astype(np.float32)
+    return sc

@@ -1,0 +1,176 @@
+"""Parity of the CUDA step with the FP64 oracle for the other switches of the
+reference (CSPM + PSE, the compensated precision form, exhaustive contact,
+tool particles with conduction) and the failure paths (NaN blanking, secant
+iteration limit), all through the C ABI."""
+import numpy as np
+import pytest
+
+import oracle
+from iwf_mfree_gpu_3d_b200 import api, scenes
+
+from helpers import compare, gpu_state, oracle_state
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(sc, steps, **opt):
+    sim = api.Simulation.from_scene(sc, **opt)
+    orc = oracle.Oracle(sc, prec=64)
+    for _ in range(steps):
+        sim.step()
+        orc.step()
+    return sim, orc
+
+
+def test_cspm_pse_100_steps():
+    """CSPM correction + PSE conduction (the 1M configuration's switches) on a
+    30 x 15 x 12 block: per-field relative L2 after 100 steps."""
+    sc = scenes.orthogonal_cutting(30, 15, 12, cspm=True, conduction=2)
+    sim, orc = _run(sc, 100)
+    err = compare(gpu_state(sim), oracle_state(orc), sc)
+    print("CSPM+PSE 100-step relative L2:", err)
+    assert err["blank_mismatch"] == 0
+    for k, v in dict(POS=5e-3, VEL=5e-3, S=5e-3, EPS_PL=2e-2, T=2e-2, RHO=5e-3).items():
+        assert err[k] < v, (k, err)
+    sim.close()
+
+
+def test_precision_form_tracks_fp64_closer():
+    """Compensated hi/lo positions and velocities: the displacement error
+    against the FP64 oracle is no worse than plain FP32's."""
+    sc = scenes.small_scene()
+    plain, orc = _run(sc, 60)
+    prec = api.Simulation.from_scene(sc, precision=1)
+    for _ in range(60):
+        prec.step()
+    o = oracle_state(orc)
+    e_plain = compare(gpu_state(plain), o, sc)
+    e_prec = compare(gpu_state(prec, f64=True), o, sc)
+    print("plain:", e_plain["POS"], e_plain["VEL"], "precision form:", e_prec["POS"], e_prec["VEL"])
+    assert e_prec["POS"] < 5e-3 and e_prec["VEL"] < 5e-3
+    assert e_prec["POS"] <= 1.5 * e_plain["POS"]
+    plain.close()
+    prec.close()
+
+
+def test_exhaustive_contact_algorithm():
+    sc = scenes.small_scene(algorithm=api.CONTACT_EXHAUSTIVE)
+    sim, orc = _run(sc, 30)
+    err = compare(gpu_state(sim), oracle_state(orc), sc)
+    print("exhaustive contact 30-step relative L2:", err)
+    for k, v in dict(POS=5e-3, VEL=5e-3, S=5e-3, FC=2e-2).items():
+        assert err[k] < v, (k, err)
+    sim.close()
+
+
+def test_tool_particles_conduct_heat():
+    """Tool particles (tool_p = 1) exchange heat by Brookshaw conduction, skip
+    the mechanics and translate with the tool (actions_gpu.cu:55-68)."""
+    sc = scenes.small_scene()
+    n = sc.n
+    # make the 200 particles with the largest x tool particles at 600 K
+    sel = np.argsort(sc.pos[:, 0])[-200:]
+    sc.tool_p[sel] = 1.0
+    sc.T[sel] = 600.0
+    sc.fixed[sel] = 0.0
+    sc.trml_tool = dict(cp=5.2e-6, tq=0.0, k=2.2e-10, alpha=2.2e-10 / (3.5 * 5.2e-6), T_init=300.0, eta=0.0)
+    sim, orc = _run(sc, 40)
+    g, o = gpu_state(sim), oracle_state(orc)
+    err = compare(g, o, sc)
+    print("tool particles 40-step relative L2:", err)
+    for k, v in dict(POS=5e-3, VEL=5e-3, T=2e-2).items():
+        assert err[k] < v, (k, err)
+    # tool particles moved rigidly with the tool velocity
+    ids = sim.get("ID")
+    pos = np.empty((n, 4), np.float32)
+    pos[ids] = sim.get("POS")
+    dxt = pos[sel, 0] - sc.pos[sel, 0]
+    assert np.allclose(dxt, dxt.mean(), atol=1e-9) and dxt.mean() < 0
+    sim.close()
+
+
+def test_nan_rate_is_blanked_and_counted():
+    """A particle whose rate is NaN is blanked at the next step and never
+    unblanked (actions_gpu.cu:506-529): it leaves the active range."""
+    sc = scenes.small_scene()
+    sim = api.Simulation.from_scene(sc)
+    sim.step()
+    vt = sim.get("VEL_T")
+    ids = sim.get("ID")
+    k = int(np.where(ids == 1234)[0][0])
+    vt[k, 0] = np.nan
+    sim.set("VEL_T", vt)
+    sim.step()
+    n_act, n_init = sim.counts()
+    assert n_act == n_init - 1
+    ids = sim.get("ID")
+    assert ids[n_init - 1] == 1234 and sim.get("BLANKED")[n_init - 1] == 1.0
+    for _ in range(3):
+        sim.step()
+    assert sim.counts()[0] == n_init - 1
+    assert sim.counters()["nan_blanked"] >= 1
+    sim.close()
+
+
+def test_velocity_blanking_moves_particle_to_tail():
+    sc = scenes.small_scene()
+    sim = api.Simulation.from_scene(sc)
+    sim.step()
+    v = sim.get("VEL")
+    ids = sim.get("ID")
+    k = int(np.where(ids == 77)[0][0])
+    v[k, 0] = 10.0  # above the 4 cm/us blanking speed
+    sim.set("VEL", v)
+    sim.step()
+    n_act, n_init = sim.counts()
+    assert n_act == n_init - 1 and sim.get("ID")[n_init - 1] == 77
+    sim.close()
+
+
+def test_secant_iteration_limit_is_reported():
+    """With the iteration limit at 1 the radial return reports failures
+    through the counters instead of printing (actions_gpu.cu:415-418)."""
+    sc = scenes.small_scene()
+    sim = api.Simulation.from_scene(sc, max_secant_iter=1)
+    for _ in range(15):
+        sim.step()
+    assert sim.counters()["secant_failures"] > 0
+    assert np.isfinite(sim.get("S")).all()
+    sim.close()
+
+
+def test_field_round_trip_and_reference_layout():
+    sc = scenes.small_scene()
+    sim = api.Simulation.from_scene(sc)
+    sim.step()
+    S = sim.get("S").reshape(-1, 3, 3)
+    np.testing.assert_array_equal(S, np.transpose(S, (0, 2, 1)))  # symmetric, GLM column-major
+    for name in ("POS", "VEL", "S", "T", "EPS_PL", "FT", "VEL_T"):
+        a = sim.get(name)
+        sim.set(name, a)
+        np.testing.assert_array_equal(sim.get(name), a)
+    assert set(sim.get("IDX")) == set(range(sc.n))
+    sim.close()
+
+
+def test_moving_grid_and_blanking_box():
+    """Locked grid and blanking box moving with a velocity (the reference's
+    moving-window setup, grid_gpu_base.cu:166-183, blanking.cpp:43-51)."""
+    sc = scenes.small_scene()
+    sim = api.Simulation.from_scene(sc)
+    orc = oracle.Oracle(sc, prec=64)
+    v = np.array([-2.0, 0.0, 0.0], np.float32)  # sweeps the box over the block quickly
+    sim.set_grid_velocity(v)
+    sim.set_blanking(sc.blank_bbmin, sc.blank_bbmax, sc.blank_vmax, bbvel=v)
+    import ctypes as C
+    oracle.lib().orc_set_grid_velocity(orc.h, v.ctypes.data_as(C.POINTER(C.c_float)))
+    oracle.lib().orc_set_blanking(orc.h, sc.blank_bbmin.ctypes.data_as(C.POINTER(C.c_float)),
+                                  sc.blank_bbmax.ctypes.data_as(C.POINTER(C.c_float)),
+                                  v.ctypes.data_as(C.POINTER(C.c_float)), sc.blank_vmax)
+    for _ in range(20):
+        sim.step()
+        orc.step()
+    assert sim.counts()[0] == orc.counts()[0] < sc.n
+    err = compare(gpu_state(sim), oracle_state(orc), sc)
+    assert err["blank_mismatch"] == 0
+    sim.close()
