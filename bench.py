@@ -242,6 +242,22 @@ def run_reference(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------- multi-process ----
+def reduce_max(dist, x: float, device: str) -> float:
+    """Max over ranks (the slowest rank's time), or x itself without a process group."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate(n_particles: int, steps: int, world: int, max_seconds: float) -> float:
+    """Whole-job particle-steps/s: every rank steps its own scene of the same size."""
+    return n_particles * steps * world / max_seconds
+
+
 # ---------------------------------------------------------------- ours ----
 def run_ours(args, rank: int, world: int, local_rank: int, dist):
     from iwf_mfree_gpu_3d_b200 import api
@@ -276,11 +292,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     ktimes = sim.kernel_times()
     counters = sim.counters()
     sim.close()
+    ms = reduce_max(dist, ms, f"cuda:{local_rank}")
     if dist:
-        import torch
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
 
     # --- end to end through the C ABI with host buffers
@@ -288,7 +301,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
 
     if rank != 0:
         return
-    value = sc.n * args.steps * world / (ms * 1e-3)
+    value = aggregate(sc.n, args.steps, world, ms * 1e-3)
     ik_ms, ik_n = ktimes["interact"]
     ik_avg = ik_ms / max(ik_n, 1)
     achieved = flops_launch / (ik_avg * 1e-3) / 1e12
@@ -363,13 +376,9 @@ def run_e2e(sc, args, opts, dist, local_rank) -> dict:
     d2h += sum(a.nbytes for a in out)
     t = time.perf_counter() - t0
     s.close()
-    if dist:
-        import torch as _t
-        tt = _t.tensor([t], dtype=_t.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t = float(tt.item())
+    t = reduce_max(dist, t, f"cuda:{local_rank}")
     world = dist.get_world_size() if dist else 1
-    return {"value": sc.n * args.steps * world / t, "unit": "particle-steps/s",
+    return {"value": aggregate(sc.n, args.steps, world, t), "unit": "particle-steps/s",
             "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
             "note": "wall clock: context creation from pinned host arrays, setup, steps with a per-step tool-force "
                     "read-back, final read-back of POS/VEL/S/T/EPS_PL; state bytes amortised over the steps"}

@@ -61,7 +61,7 @@ typedef struct {
     int precision;          /* 0: FP32 state; 1: FP32 bulk + compensated hi/lo
                                position and velocity in predictor/corrector          */
     int max_secant_iter;    /* Johnson-Cook secant limit (plasticity.cuh:66: 100)     */
-    int lanes_per_particle; /* interaction tiling: 4, 8, 16 or 32 lanes of a warp per
+    int lanes_per_particle; /* pair-loop tiling: 8, 16 or 32 lanes of a warp per
                                particle; 0 picks the tuned default                   */
     int diagnostics;        /* 1: keep neighbour counts, half-step positions and
                                contact normals for mfree_get_field()                  */

@@ -15,11 +15,13 @@
 //   The deviatoric stress is symmetric in the reference (every writer keeps
 //   S[c][r] == S[r][c]: predict/correct element-wise, Jaumann
 //   omega*S + S*omega^T, radial return), so 6 components are stored.
-//   half-step neighbour records, written by the predictor in sorted order and
-//   read by the pair loop:
-//     nP = (x, y, z, tool_flag)      nV = (vx, vy, vz, rho)
-//     nA = sigma(xx, yy, zz, xy)     nB = (sigma_xz, sigma_yz, c = sqrt(K/rho), h)
-//     nR = R(xx, yy, zz, xy)         nC = (R_xz, R_yz, T, m/rho)
+//   half-step neighbour records (one 96-byte record per particle, in sorted
+//   order, written by the predictor and read by the pair loop; a halo column
+//   of records is one contiguous range, staged into shared memory by a single
+//   bulk copy):
+//     P = (x, y, z, tool_flag)      V = (vx, vy, vz, rho)
+//     A = sigma(xx, yy, zz, xy)     B = (sigma_xz, sigma_yz, c = sqrt(K/rho), h)
+//     R = R(xx, yy, zz, xy)         C = (R_xz, R_yz, T, m/rho)
 //   with sigma = (S - p I)/rho^2 (the per-particle factor of the stress
 //   divergence, interactions_gpu.cu:389-399) and R the artificial stress.
 #pragma once
@@ -43,6 +45,8 @@ struct DevClock {
     int pending;      // 1 once a step has run: the next clock tick adds dt first
     int n_active;     // N (particles not blanked), written by the scan
     int record;       // record tool forces this step
+    int tile_next;    // work queue of the pair kernel (reset by the clock kernel)
+    int tile_error;   // staging waits that ran out (the tile fell back to global reads)
     long long step_index;
     float blank_min[3], blank_max[3];
     float grid_min[3];
@@ -99,8 +103,13 @@ struct State {
     float4 *pos4, *vel4, *sa4, *sb4, *da4, *dv4, *dsa4, *dsb4, *fc4, *ft4, *bc4, *lo4, *lo4b;
 };
 
+struct __align__(16) Rec {
+    float4 P, V, A, B, R, C;
+};
+static_assert(sizeof(Rec) == 96, "neighbour record must be 96 bytes");
+
 struct Records {
-    float4 *P, *V, *A, *B, *R, *C;
+    Rec *rec;
 };
 
 struct Scratch {

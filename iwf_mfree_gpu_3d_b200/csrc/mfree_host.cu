@@ -284,11 +284,16 @@ int ready(mfree_ctx *c) {
     if (c->phys.mass <= 0.f || c->phys.rho0 <= 0.f) return fail(MFREE_ERR_ARG, "mfree_set_physics: mass and rho0 must be > 0");
     if (c->tools.size() > size_t(MAX_TOOLS)) return fail(MFREE_ERR_ARG, "too many tools");
     int lpp = c->opt.lanes_per_particle;
-    if (lpp != 0 && lpp != 4 && lpp != 8 && lpp != 16 && lpp != 32)
-        return fail(MFREE_ERR_ARG, "lanes_per_particle must be 0, 4, 8, 16 or 32");
+    if (lpp != 0 && lpp != 8 && lpp != 16 && lpp != 32)
+        return fail(MFREE_ERR_ARG, "lanes_per_particle must be 0, 8, 16 or 32");
     if (c->opt.conduction < 0 || c->opt.conduction > 2) return fail(MFREE_ERR_ARG, "bad conduction mode");
     int st = ensure_scratch(c);
     if (st) return st;
+    {
+        StepArgs a = make_args(c);
+        cudaError_t e = launch_interact(a, lpp ? lpp : default_lpp(), 0, c->stream);
+        if (e != cudaSuccess) return fail(MFREE_ERR_CUDA, std::string("pair kernel setup: ") + cudaGetErrorString(e));
+    }
     if (c->clock_dirty) return write_clock(c);
     return MFREE_OK;
 }
@@ -342,6 +347,13 @@ int enqueue_step(mfree_ctx *c, int record_mode, int record_every, bool timed = f
     return MFREE_OK;
 }
 
+int copy_records(mfree_ctx *c, std::vector<Rec> &dst) {
+    dst.resize(c->n_init);
+    CUDA_TRY(cudaMemcpyAsync(dst.data(), c->rec.rec, sizeof(Rec) * c->n_init, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return MFREE_OK;
+}
+
 int copy_field_raw(mfree_ctx *c, const float4 *src, std::vector<float4> &dst) {
     dst.resize(c->n_init);
     CUDA_TRY(cudaMemcpyAsync(dst.data(), src, sizeof(float4) * c->n_init, cudaMemcpyDeviceToHost, c->stream));
@@ -380,9 +392,7 @@ int mfree_create(int n, const float *pos4, const float *vel4, const float *rho, 
         for (auto p : f)
             if ((st = dalloc(c.get(), p, n, L))) return st;
     }
-    float4 **r[] = {&c->rec.P, &c->rec.V, &c->rec.A, &c->rec.B, &c->rec.R, &c->rec.C};
-    for (auto p : r)
-        if ((st = dalloc(c.get(), p, n, L))) return st;
+    if ((st = dalloc(c.get(), &c->rec.rec, n, L))) return st;
     if ((st = dalloc(c.get(), &c->scr.key, n, L))) return st;
     if ((st = dalloc(c.get(), &c->scr.key_sorted, n, L))) return st;
     if ((st = dalloc(c.get(), &c->scr.perm, n, L))) return st;
@@ -431,7 +441,7 @@ int mfree_create(int n, const float *pos4, const float *vel4, const float *rho, 
     CUDA_TRY(up(S.bc4, hbc));
     CUDA_TRY(up(S.lo4, hz));
     CUDA_TRY(up(S.lo4b, hz));
-    for (auto p : r) CUDA_TRY(up(*p, hz));
+    CUDA_TRY(cudaMemsetAsync(c->rec.rec, 0, sizeof(Rec) * n, c->stream));
     CUDA_TRY(cudaMemcpyAsync(c->scr.perm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(cudaMemsetAsync(c->scr.key_sorted, 0, sizeof(int) * n, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -886,15 +896,13 @@ int get_field_impl(mfree_ctx *c, int f, float *fo, double *dout) {
             CUDA_TRY(cudaStreamSynchronize(c->stream));
             for (int i = 0; i < n; i++) put(i, 0, A[i].w);
             break;
-        case MFREE_P:
-            if ((st = copy_field_raw(c, c->rec.V, A))) return st;
-            if ((st = copy_field_raw(c, S.fc4, B))) return st;
-            CUDA_TRY(cudaStreamSynchronize(c->stream));
-            {
-                float c0 = std::sqrt(c->phys.rho0 != 0.f ? c->phys.K / c->phys.rho0 : 0.f);
-                for (int i = 0; i < n; i++) put(i, 0, B[i].w == 1.f ? 0.f : c0 * c0 * (A[i].w - c->phys.rho0));
-            }
+        case MFREE_P: {
+            std::vector<Rec> R;
+            if ((st = copy_records(c, R))) return st;
+            float c0 = std::sqrt(c->phys.rho0 != 0.f ? c->phys.K / c->phys.rho0 : 0.f);
+            for (int i = 0; i < n; i++) put(i, 0, R[i].P.w == 1.f ? 0.f : c0 * c0 * (R[i].V.w - c->phys.rho0));
             break;
+        }
         case MFREE_S:
         case MFREE_S_T: {
             if ((st = copy_field_raw(c, f == MFREE_S ? S.sa4 : S.dsa4, A))) return st;
@@ -906,15 +914,15 @@ int get_field_impl(mfree_ctx *c, int f, float *fo, double *dout) {
             }
             break;
         }
-        case MFREE_R:
-            if ((st = copy_field_raw(c, c->rec.R, A))) return st;
-            if ((st = copy_field_raw(c, c->rec.C, B))) return st;
-            CUDA_TRY(cudaStreamSynchronize(c->stream));
+        case MFREE_R: {
+            std::vector<Rec> R;
+            if ((st = copy_records(c, R))) return st;
             for (int i = 0; i < n; i++) {
-                float s6[6] = {A[i].x, A[i].y, A[i].z, A[i].w, B[i].x, B[i].y};
+                float s6[6] = {R[i].R.x, R[i].R.y, R[i].R.z, R[i].R.w, R[i].C.x, R[i].C.y};
                 sym_to_9(s6, &tmp[size_t(i) * 9]);
             }
             break;
+        }
         case MFREE_FC:
         case MFREE_FT:
         case MFREE_POS_T:

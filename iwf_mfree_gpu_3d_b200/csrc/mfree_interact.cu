@@ -13,29 +13,23 @@
 //                             leap_frog.cu:102-119, actions_gpu.cu:55-68,451-487
 //                             (particles inside a tool box defer these to k_finalize)
 //
-// Work decomposition: a warp owns 32 consecutive sorted particles.  It walks
-// them in LPP rounds; in each round every group of LPP lanes serves one
-// particle.  The 5x5x5 cell stencil is read as 25 contiguous particle ranges
-// (five consecutive z cells of one (x, y) column are consecutive in the sorted
-// order).  Pass A streams all candidates through the lanes: it tests the
-// support, accumulates PSE (which sums every stencil candidate) and the CSPM
-// matrix, and compacts the in-support neighbours into a shared-memory queue
-// with a ballot.  Pass B runs the full pair body on the queue only -- the
-// reference evaluates every candidate, ~3.5x more work, and candidates outside
-// the support contribute exact zeros there.  Accumulators are reduced across
-// the group with xor shuffles; after the LPP rounds each lane runs the
-// per-particle epilogue for one particle.
+// Work decomposition: a persistent block (512 threads, one per SM) pulls
+// tiles of 4 x 4 x 6 cells from a work counter.  The tile's particles are 16
+// contiguous ranges of the sorted order; the records their 5x5x5 stencils
+// touch are the 64 contiguous column ranges of the 8 x 8 x 10-cell halo,
+// staged into shared memory with one bulk copy per column (TMA
+// cp.async.bulk, completion counted on an mbarrier, bounded waits).  Each
+// target is served by a group of LPP lanes.  Pass A streams the target's
+// candidates (25 column ranges of the staged halo) through the lanes: support
+// test, PSE (which sums every stencil candidate), CSPM matrix, and a ballot
+// that compacts the in-support neighbours into a queue.  Pass B runs the full
+// pair body on the queue only -- the reference evaluates every candidate,
+// ~3.5x more work, and candidates outside the support contribute exact zeros
+// there.  Accumulators are reduced across the group with xor shuffles; then
+// one thread per target runs the per-particle epilogue.
 #include "mfree_kernels.cuh"
 
 namespace mfree {
-
-template <int LPP> struct WarpSmem {
-    static constexpr int G = 32 / LPP;
-    int cbase[G][25];
-    int cpref[G][26];
-    int q[G][QCAP];
-    float res[32][NRES + 1];
-};
 
 // 2x2 minors of the column-major (GLM) 3x3 in m[c*3+r]
 __device__ __forceinline__ float det3(const float *m) {
@@ -289,192 +283,363 @@ __device__ void epilogue(const StepArgs &a, int i, const float *res) {
 }
 
 // ---------------------------------------------------------- pair kernel --
+// Tile = TX x TY x TZ cells of the cell grid; its particles are 16 contiguous
+// column ranges of the sorted order.  Their 5x5x5 stencils lie in the halo of
+// HX x HY x HZ cells, i.e. 64 contiguous column ranges of neighbour records,
+// which one bulk copy each (cp.async.bulk, completion on an mbarrier) stages
+// into shared memory.  A tile whose halo exceeds the staging capacity reads
+// the same records from global memory instead.
+constexpr int TX = 4, TY = 4, TZ = 6;
+constexpr int HX = TX + 4, HY = TY + 4, HZ = TZ + 4;
+constexpr int NHC = HX * HY;           // halo columns
+constexpr int NTC = TX * TY;           // target columns
+constexpr int TILE_THREADS = 512;
+constexpr int TILE_WARPS = TILE_THREADS / 32;
+constexpr int TCAP = 256;              // targets per pass of a tile
+constexpr int QCAP_T = 96;             // in-support queue per target before the rescan path
+constexpr int SMEM_LIMIT = 232448;     // per-block shared memory of sm_100
+
+template <int LPP> struct TileSmem {
+    static constexpr int G = 32 / LPP;
+    float res[TCAP][NRES + 1];
+    int q[TILE_WARPS][G][QCAP_T];
+    int cbase[TILE_WARPS][G][25];
+    int cpref[TILE_WARPS][G][26];
+    int cellstart[NHC][HZ + 1];
+    int hoff[NHC];       // staged offset of halo column
+    int hstart[NHC];     // global start of halo column
+    int tstart[NTC];
+    int tpref[NTC + 1];
+    unsigned long long bar;
+    int tile, total, staged, parity;
+};
+template <int LPP> __host__ __device__ constexpr int rec_capacity() {
+    return int((SMEM_LIMIT - sizeof(TileSmem<LPP>) - 256) / sizeof(Rec));
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return unsigned(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ void mbar_init(unsigned long long *b, unsigned n) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(n) : "memory");
+}
+__device__ __forceinline__ void mbar_expect(unsigned long long *b, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(unsigned long long *b, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void bulk_to_smem(void *dst, const void *src, unsigned bytes, unsigned long long *b) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(b))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 template <int LPP, bool CSPM, int COND, bool PREC>
-__global__ void __launch_bounds__(INTERACT_WARPS * 32) k_interact(StepArgs a) {
+__global__ void __launch_bounds__(TILE_THREADS, 1) k_interact(StepArgs a, int ntx, int nty, int ntz) {
     constexpr int G = 32 / LPP;
-    __shared__ WarpSmem<LPP> smem[INTERACT_WARPS];
+    constexpr int CAP = rec_capacity<LPP>();
+    extern __shared__ __align__(128) unsigned char dyn[];
+    TileSmem<LPP> &sm = *reinterpret_cast<TileSmem<LPP> *>(dyn);
+    Rec *srec = reinterpret_cast<Rec *>(dyn + ((sizeof(TileSmem<LPP>) + 127) / 128) * 128);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane / LPP, sl = lane - g * LPP;
-    WarpSmem<LPP> &sm = smem[warp];
-    const Params &P = a.p;
-    const int N = a.clk->n_active;
-    const int nbatch = (N + 31) >> 5;
     const unsigned lt_mask = (1u << lane) - 1u;
     const unsigned gmask = LPP == 32 ? 0xffffffffu : (((1u << LPP) - 1u) << (g * LPP));
+    const Params &P = a.p;
     const int nx = P.gnx, ny = P.gny, nz = P.gnz;
-    const float4 *__restrict__ RP = a.r.P;
-    const float4 *__restrict__ RV = a.r.V;
-    const float4 *__restrict__ RA = a.r.A;
-    const float4 *__restrict__ RB = a.r.B;
-    const float4 *__restrict__ RR = a.r.R;
-    const float4 *__restrict__ RC = a.r.C;
     const int *__restrict__ first = a.s.first;
-
-    for (int batch = blockIdx.x * INTERACT_WARPS + warp; batch < nbatch; batch += gridDim.x * INTERACT_WARPS) {
-        const int base = batch << 5;
+    const Rec *__restrict__ grec = a.r.rec;
+    const int ntiles = ntx * nty * ntz;
+    if (threadIdx.x == 0) {
+        mbar_init(&sm.bar, 1);
+        sm.parity = 0;
+    }
+    fence_proxy_async();
+    __syncthreads();
+    for (;;) {
+        if (threadIdx.x == 0) sm.tile = atomicAdd(&a.clk->tile_next, 1);
+        __syncthreads();
+        const int tile = sm.tile;
+        if (tile >= ntiles) break;
+        const int tz = tile % ntz, txy = tile / ntz, ty = txy % nty, tx = txy / nty;
+        const int X0 = tx * TX, Y0 = ty * TY, Z0 = tz * TZ;
+        const int zl = max(Z0 - 2, 0), zh = min(Z0 + TZ + 1, nz - 1);
+        const int nzr = zh - zl + 2;  // cell starts per halo column (inclusive end)
+        // ---- tables: halo cell starts and target ranges
+        for (int e = threadIdx.x; e < NHC * (HZ + 1); e += TILE_THREADS) {
+            const int c = e / (HZ + 1), k = e - c * (HZ + 1);
+            const int cx = X0 - 2 + c / HY, cy = Y0 - 2 + c % HY;
+            int v = 0;
+            if (k < nzr && cx >= 0 && cx < nx && cy >= 0 && cy < ny) v = first[(cx * ny + cy) * nz + zl + k];
+            sm.cellstart[c][k] = v;
+        }
+        if (threadIdx.x < NTC) {
+            const int c = threadIdx.x;
+            const int cx = X0 + c / TY, cy = Y0 + c % TY;
+            int s0 = 0, len = 0;
+            if (cx < nx && cy < ny && Z0 < nz) {
+                const int cb = (cx * ny + cy) * nz;
+                s0 = first[cb + Z0];
+                len = first[cb + min(Z0 + TZ - 1, nz - 1) + 1] - s0;
+            }
+            sm.tstart[c] = s0;
+            sm.tpref[c] = len;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int acc = 0;
+            for (int c = 0; c < NTC; c++) {
+                const int l = sm.tpref[c];
+                sm.tpref[c] = acc;
+                acc += l;
+            }
+            sm.tpref[NTC] = acc;
+            int tot = 0;
+            for (int c = 0; c < NHC; c++) {
+                sm.hstart[c] = sm.cellstart[c][0];
+                sm.hoff[c] = tot;
+                const int cx = X0 - 2 + c / HY, cy = Y0 - 2 + c % HY;
+                if (cx >= 0 && cx < nx && cy >= 0 && cy < ny) tot += sm.cellstart[c][nzr - 1] - sm.cellstart[c][0];
+            }
+            sm.total = tot;
+            sm.staged = (acc > 0 && tot <= CAP) ? 1 : 0;
+            if (sm.staged && tot > 0) mbar_expect(&sm.bar, unsigned(tot) * unsigned(sizeof(Rec)));
+        }
+        __syncthreads();
+        const int T = sm.tpref[NTC];
+        if (T == 0) continue;  // (the loop head synchronises before the next tile)
+        const bool staged = sm.staged != 0;
+        if (staged && sm.total > 0) {
+            if (threadIdx.x < NHC) {
+                const int c = threadIdx.x;
+                const int cx = X0 - 2 + c / HY, cy = Y0 - 2 + c % HY;
+                if (cx >= 0 && cx < nx && cy >= 0 && cy < ny) {
+                    const int len = sm.cellstart[c][nzr - 1] - sm.cellstart[c][0];
+                    if (len > 0)
+                        bulk_to_smem(srec + sm.hoff[c], grec + sm.hstart[c], unsigned(len) * unsigned(sizeof(Rec)),
+                                     &sm.bar);
+                }
+            }
+            // bounded wait for the staged halo
+            const unsigned par = unsigned(sm.parity);
+            unsigned it = 0;
+            bool ok = true;
+            while (!mbar_try(&sm.bar, par)) {
+                if (++it > (1u << 22)) {
+                    ok = false;
+                    break;
+                }
+            }
+            if (!__syncthreads_and(ok)) {
+                // the copies did not complete in time: record it, wait once more
+                // (bounded) for them to land, and leave the kernel
+                if (threadIdx.x == 0) atomicAdd(&a.clk->tile_error, 1);
+                unsigned it2 = 0;
+                while (!mbar_try(&sm.bar, par) && ++it2 < (1u << 22)) {
+                }
+                return;
+            }
+            if (threadIdx.x == 0) sm.parity ^= 1;
+        }
+        const Rec *R = staged ? srec : grec;
+        // ---- targets, TCAP per pass
+        for (int t0 = 0; t0 < T; t0 += TCAP) {
+            const int tn = min(TCAP, T - t0);
+            const int rounds = (tn + TILE_WARPS * G - 1) / (TILE_WARPS * G);
 #pragma unroll 1
-        for (int rnd = 0; rnd < LPP; rnd++) {
-            const int i = base + rnd * G + g;
-            const bool valid = i < N;
-            const int ii = valid ? i : base;
-            IData I;
-            {
-                const float4 Pi = RP[ii], Vi = RV[ii], Ai = RA[ii], Bi = RB[ii], Ri = RR[ii], Ci = RC[ii];
-                I.x = Pi.x; I.y = Pi.y; I.z = Pi.z; I.tool = Pi.w;
-                I.vx = Vi.x; I.vy = Vi.y; I.vz = Vi.z; I.rho = Vi.w;
-                I.s[0] = Ai.x; I.s[1] = Ai.y; I.s[2] = Ai.z; I.s[3] = Ai.w; I.s[4] = Bi.x; I.s[5] = Bi.y;
-                I.c = Bi.z; I.h = Bi.w;
-                I.R[0] = Ri.x; I.R[1] = Ri.y; I.R[2] = Ri.z; I.R[3] = Ri.w; I.R[4] = Ci.x; I.R[5] = Ci.y;
-                I.T = Ci.z;
-                I.h1 = 1.0f / I.h;
-                I.fac = 0.31830988618379067f * I.h1 * I.h1 * I.h1;
-            }
-            // the 25 (x, y) columns of the 5x5x5 stencil around the particle's cell
-            {
-                const unsigned key = a.s.key_sorted[ii];
-                const int nyz = ny * nz;
-                const int gi = int(key) / nyz, rem = int(key) - gi * nyz, gj = rem / nz, gk = rem - gj * nz;
-                const int z0 = max(gk - 2, 0), z1 = min(gk + 2, nz - 1);
-                for (int c = sl; c < 25; c += LPP) {
-                    const int cx = gi + c / 5 - 2, cy = gj + c % 5 - 2;
-                    int s = 0, e = 0;
-                    if (valid && cx >= 0 && cx < nx && cy >= 0 && cy < ny) {
-                        const int cb = (cx * ny + cy) * nz;
-                        s = first[cb + z0];
-                        e = first[cb + z1 + 1];
-                    }
-                    sm.cbase[g][c] = s;
-                    sm.cpref[g][c] = e - s;
+            for (int rnd = 0; rnd < rounds; rnd++) {
+                const int tt = rnd * TILE_WARPS * G + warp * G + g;  // target slot in this pass
+                const bool valid = tt < tn;
+                int i = 0;
+                {
+                    const int tg = t0 + (valid ? tt : 0);
+                    int c = 0;
+                    while (c < NTC - 1 && sm.tpref[c + 1] <= tg) c++;
+                    i = sm.tstart[c] + (tg - sm.tpref[c]);
                 }
-            }
-            __syncwarp();
-            if (sl == 0) {
-                int acc = 0;
-                for (int c = 0; c < 25; c++) {
-                    const int l = sm.cpref[g][c];
-                    sm.cpref[g][c] = acc;
-                    acc += l;
+                const Rec &Ri = grec[i];
+                IData I;
+                {
+                    const float4 Pi = Ri.P, Vi = Ri.V, Ai = Ri.A, Bi = Ri.B, RRi = Ri.R, Ci = Ri.C;
+                    I.x = Pi.x; I.y = Pi.y; I.z = Pi.z; I.tool = Pi.w;
+                    I.vx = Vi.x; I.vy = Vi.y; I.vz = Vi.z; I.rho = Vi.w;
+                    I.s[0] = Ai.x; I.s[1] = Ai.y; I.s[2] = Ai.z; I.s[3] = Ai.w; I.s[4] = Bi.x; I.s[5] = Bi.y;
+                    I.c = Bi.z; I.h = Bi.w;
+                    I.R[0] = RRi.x; I.R[1] = RRi.y; I.R[2] = RRi.z; I.R[3] = RRi.w; I.R[4] = Ci.x; I.R[5] = Ci.y;
+                    I.T = Ci.z;
+                    I.h1 = 1.0f / I.h;
+                    I.fac = 0.31830988618379067f * I.h1 * I.h1 * I.h1;
                 }
-                sm.cpref[g][25] = acc;
-            }
-            __syncwarp();
-            const int total = sm.cpref[g][25];
-            int maxtotal = total;
-#pragma unroll
-            for (int o = 16; o >= LPP; o >>= 1) maxtotal = max(maxtotal, __shfl_xor_sync(0xffffffffu, maxtotal, o));
-
-            // ---- pass A: support test, PSE, CSPM matrix, queue
-            const float inv_h2 = I.h1 * I.h1;
-            int col = 0, qn = 0, cnt = 0;
-            float pse = 0.f;
-            float Bm[9];
-#pragma unroll
-            for (int k = 0; k < 9; k++) Bm[k] = 0.f;
-            for (int k0 = 0; k0 < maxtotal; k0 += LPP) {
-                const int k = k0 + sl;
-                bool ins = false;
-                int j = 0;
-                if (k < total) {
-                    while (sm.cpref[g][col + 1] <= k) col++;
-                    j = sm.cbase[g][col] + (k - sm.cpref[g][col]);
-                    const float4 Pj = RP[j];
-                    const float dx = I.x - Pj.x, dy = I.y - Pj.y, dz = I.z - Pj.z;
-                    const float r2 = dist2_rn(dx, dy, dz);
-                    ins = in_support(r2, I.h);
-                    if (COND == MFREE_COND_PSE || CSPM) {
-                        const float4 Cj = RC[j];
-                        if (COND == MFREE_COND_PSE) pse = fmaf((Cj.z - I.T) * Cj.w, __expf(-r2 * inv_h2), pse);
-                        if (CSPM && ins && !(I.tool == 1.f) && !(Pj.w == 1.f)) {
-                            float w, dfac;
-                            spline(r2, I.h1, I.fac, w, dfac);
-                            const float d[3] = {dx, dy, dz};
-                            const float gr[3] = {dfac * dx, dfac * dy, dfac * dz};
-#pragma unroll
-                            for (int c = 0; c < 3; c++)
-#pragma unroll
-                                for (int r = 0; r < 3; r++) Bm[c * 3 + r] = fmaf(-Cj.w * d[r], gr[c], Bm[c * 3 + r]);
+                // stencil columns of this target as ranges of R
+                {
+                    const unsigned key = a.s.key_sorted[i];
+                    const int nyz = ny * nz;
+                    const int gi = int(key) / nyz, rem = int(key) - gi * nyz, gj = rem / nz, gk = rem - gj * nz;
+                    const int klo = max(gk - 2, 0) - zl, khi = min(gk + 2, nz - 1) - zl + 1;
+                    for (int c = sl; c < 25; c += LPP) {
+                        const int cx = gi + c / 5 - 2, cy = gj + c % 5 - 2;
+                        int b = 0, l = 0;
+                        if (valid && cx >= 0 && cx < nx && cy >= 0 && cy < ny) {
+                            const int lc = (cx - X0 + 2) * HY + (cy - Y0 + 2);
+                            const int s0 = sm.cellstart[lc][klo];
+                            l = sm.cellstart[lc][khi] - s0;
+                            b = staged ? sm.hoff[lc] + (s0 - sm.hstart[lc]) : s0;
                         }
+                        sm.cbase[warp][g][c] = b;
+                        sm.cpref[warp][g][c] = l;
                     }
                 }
-                cnt += ins ? 1 : 0;
-                const unsigned m = __ballot_sync(0xffffffffu, ins) & gmask;
-                if (ins) {
-                    const int pos = qn + __popc(m & lt_mask);
-                    if (pos < QCAP) sm.q[g][pos] = j;
+                __syncwarp();
+                if (sl == 0) {
+                    int acc = 0;
+                    for (int c = 0; c < 25; c++) {
+                        const int l = sm.cpref[warp][g][c];
+                        sm.cpref[warp][g][c] = acc;
+                        acc += l;
+                    }
+                    sm.cpref[warp][g][25] = acc;
                 }
-                qn += __popc(m);
-            }
-            __syncwarp();
-            float invB[9] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};
-            if (CSPM) {
+                __syncwarp();
+                const int total = sm.cpref[warp][g][25];
+                int maxtotal = total;
 #pragma unroll
-                for (int o = LPP / 2; o >= 1; o >>= 1)
+                for (int o = 16; o >= LPP; o >>= 1)
+                    maxtotal = max(maxtotal, __shfl_xor_sync(0xffffffffu, maxtotal, o));
+                const int *cb = sm.cbase[warp][g];
+                const int *cp = sm.cpref[warp][g];
+                int *qq = sm.q[warp][g];
+                // ---- pass A: support test, PSE, CSPM matrix, queue
+                const float inv_h2 = I.h1 * I.h1;
+                int col = 0, qn = 0, cnt = 0;
+                float pse = 0.f;
+                float Bm[9];
 #pragma unroll
-                    for (int k = 0; k < 9; k++) Bm[k] += __shfl_xor_sync(0xffffffffu, Bm[k], o);
-                const float det = det3(Bm);
-                if (det > 9.99999994e-9f) inv3(Bm, det, invB);
-            }
-            // ---- pass B: pair body on the in-support queue
-            float acc[19];
-#pragma unroll
-            for (int k = 0; k < 19; k++) acc[k] = 0.f;
-            const int qv = min(qn, QCAP);
-            int maxq = qv;
-#pragma unroll
-            for (int o = 16; o >= LPP; o >>= 1) maxq = max(maxq, __shfl_xor_sync(0xffffffffu, maxq, o));
-            for (int q0 = 0; q0 < maxq; q0 += LPP) {
-                const int q = q0 + sl;
-                if (q < qv) {
-                    const int j = sm.q[g][q];
-                    pair_body<CSPM, COND>(P, I, invB, RP[j], RV[j], RA[j], RB[j], RR[j], RC[j], acc);
-                }
-            }
-            // more in-support neighbours than the queue holds: rescan, take the rest
-            if (__any_sync(0xffffffffu, qn > QCAP)) {
-                int col2 = 0, ord = 0;
+                for (int k = 0; k < 9; k++) Bm[k] = 0.f;
                 for (int k0 = 0; k0 < maxtotal; k0 += LPP) {
                     const int k = k0 + sl;
                     bool ins = false;
                     int j = 0;
-                    if (k < total && qn > QCAP) {
-                        while (sm.cpref[g][col2 + 1] <= k) col2++;
-                        j = sm.cbase[g][col2] + (k - sm.cpref[g][col2]);
-                        const float4 Pj = RP[j];
-                        ins = in_support(dist2_rn(I.x - Pj.x, I.y - Pj.y, I.z - Pj.z), I.h);
+                    if (k < total) {
+                        while (cp[col + 1] <= k) col++;
+                        j = cb[col] + (k - cp[col]);
+                        const float4 Pj = R[j].P;
+                        const float dx = I.x - Pj.x, dy = I.y - Pj.y, dz = I.z - Pj.z;
+                        const float r2 = dist2_rn(dx, dy, dz);
+                        ins = in_support(r2, I.h);
+                        if (COND == MFREE_COND_PSE || CSPM) {
+                            const float4 Cj = R[j].C;
+                            if (COND == MFREE_COND_PSE) pse = fmaf((Cj.z - I.T) * Cj.w, __expf(-r2 * inv_h2), pse);
+                            if (CSPM && ins && !(I.tool == 1.f) && !(Pj.w == 1.f)) {
+                                float w, dfac;
+                                spline(r2, I.h1, I.fac, w, dfac);
+                                const float d[3] = {dx, dy, dz};
+                                const float gr[3] = {dfac * dx, dfac * dy, dfac * dz};
+#pragma unroll
+                                for (int c = 0; c < 3; c++)
+#pragma unroll
+                                    for (int r = 0; r < 3; r++) Bm[c * 3 + r] = fmaf(-Cj.w * d[r], gr[c], Bm[c * 3 + r]);
+                            }
+                        }
                     }
+                    cnt += ins ? 1 : 0;
                     const unsigned m = __ballot_sync(0xffffffffu, ins) & gmask;
-                    const int pos = ord + __popc(m & lt_mask);
-                    if (ins && pos >= QCAP)
-                        pair_body<CSPM, COND>(P, I, invB, RP[j], RV[j], RA[j], RB[j], RR[j], RC[j], acc);
-                    ord += __popc(m);
+                    if (ins) {
+                        const int pos = qn + __popc(m & lt_mask);
+                        if (pos < QCAP_T) qq[pos] = j;
+                    }
+                    qn += __popc(m);
                 }
-            }
-            if (COND == MFREE_COND_PSE) acc[18] = pse;
-            // ---- reduce over the group's lanes
+                __syncwarp();
+                float invB[9] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};
+                if (CSPM) {
 #pragma unroll
-            for (int o = LPP / 2; o >= 1; o >>= 1) {
+                    for (int o = LPP / 2; o >= 1; o >>= 1)
 #pragma unroll
-                for (int k = 0; k < 19; k++) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
-                cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-            }
-            if (sl == 0) {
-                float *rs = sm.res[rnd * G + g];
+                        for (int k = 0; k < 9; k++) Bm[k] += __shfl_xor_sync(0xffffffffu, Bm[k], o);
+                    const float det = det3(Bm);
+                    if (det > 9.99999994e-9f) inv3(Bm, det, invB);
+                }
+                // ---- pass B: pair body on the in-support queue
+                float acc[19];
 #pragma unroll
-                for (int k = 0; k < 19; k++) rs[k] = acc[k];
-                rs[19] = __int_as_float(cnt);
+                for (int k = 0; k < 19; k++) acc[k] = 0.f;
+                const int qv = min(qn, QCAP_T);
+                int maxq = qv;
+#pragma unroll
+                for (int o = 16; o >= LPP; o >>= 1) maxq = max(maxq, __shfl_xor_sync(0xffffffffu, maxq, o));
+                for (int q0 = 0; q0 < maxq; q0 += LPP) {
+                    const int q = q0 + sl;
+                    if (q < qv) {
+                        const Rec &Rj = R[qq[q]];
+                        pair_body<CSPM, COND>(P, I, invB, Rj.P, Rj.V, Rj.A, Rj.B, Rj.R, Rj.C, acc);
+                    }
+                }
+                if (__any_sync(0xffffffffu, qn > QCAP_T)) {
+                    int col2 = 0, ord = 0;
+                    for (int k0 = 0; k0 < maxtotal; k0 += LPP) {
+                        const int k = k0 + sl;
+                        bool ins = false;
+                        int j = 0;
+                        if (k < total && qn > QCAP_T) {
+                            while (cp[col2 + 1] <= k) col2++;
+                            j = cb[col2] + (k - cp[col2]);
+                            const float4 Pj = R[j].P;
+                            ins = in_support(dist2_rn(I.x - Pj.x, I.y - Pj.y, I.z - Pj.z), I.h);
+                        }
+                        const unsigned m = __ballot_sync(0xffffffffu, ins) & gmask;
+                        const int pos = ord + __popc(m & lt_mask);
+                        if (ins && pos >= QCAP_T) {
+                            const Rec &Rj = R[j];
+                            pair_body<CSPM, COND>(P, I, invB, Rj.P, Rj.V, Rj.A, Rj.B, Rj.R, Rj.C, acc);
+                        }
+                        ord += __popc(m);
+                    }
+                }
+                if (COND == MFREE_COND_PSE) acc[18] = pse;
+#pragma unroll
+                for (int o = LPP / 2; o >= 1; o >>= 1) {
+#pragma unroll
+                    for (int k = 0; k < 19; k++) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+                    cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+                }
+                if (sl == 0 && valid) {
+                    float *rs = sm.res[tt];
+#pragma unroll
+                    for (int k = 0; k < 19; k++) rs[k] = acc[k];
+                    rs[19] = __int_as_float(cnt);
+                }
+                __syncwarp();
             }
-            __syncwarp();
+            __syncthreads();
+            // ---- per-particle rest of the step, one thread per target
+            for (int tt = threadIdx.x; tt < tn; tt += TILE_THREADS) {
+                const int tg = t0 + tt;
+                int c = 0;
+                while (c < NTC - 1 && sm.tpref[c + 1] <= tg) c++;
+                epilogue<PREC, COND>(a, sm.tstart[c] + (tg - sm.tpref[c]), sm.res[tt]);
+            }
+            __syncthreads();
         }
-        const int i = base + lane;
-        if (i < N) epilogue<PREC, COND>(a, i, sm.res[lane]);
-        __syncwarp();
+        fence_proxy_async();  // generic reads of the staged halo precede the next tile's bulk writes
     }
 }
 
 // ------------------------------------------------------------ dispatch --
 template <int LPP, bool CSPM, int COND, bool PREC>
 static cudaError_t launch_one(const StepArgs &a, int grid, cudaStream_t s) {
-    k_interact<LPP, CSPM, COND, PREC><<<grid, INTERACT_WARPS * 32, 0, s>>>(a);
+    auto kern = k_interact<LPP, CSPM, COND, PREC>;
+    const int smem = SMEM_LIMIT;
+    if (grid <= 0)  // prepare only: raise the shared-memory limit (outside any graph capture)
+        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const int ntx = (a.p.gnx + TX - 1) / TX, nty = (a.p.gny + TY - 1) / TY, ntz = (a.p.gnz + TZ - 1) / TZ;
+    kern<<<grid, TILE_THREADS, smem, s>>>(a, ntx, nty, ntz);
     return cudaGetLastError();
 }
 
@@ -502,7 +667,6 @@ static cudaError_t launch_lpp(const StepArgs &a, int grid, cudaStream_t s) {
 
 cudaError_t launch_interact(const StepArgs &a, int lpp, int grid, cudaStream_t s) {
     switch (lpp) {
-        case 4: return launch_lpp<4>(a, grid, s);
         case 8: return launch_lpp<8>(a, grid, s);
         case 16: return launch_lpp<16>(a, grid, s);
         case 32: return launch_lpp<32>(a, grid, s);
@@ -510,14 +674,11 @@ cudaError_t launch_interact(const StepArgs &a, int lpp, int grid, cudaStream_t s
     }
 }
 
-// persistent-style grid: enough blocks to fill every SM several times over,
-// never more than there are 32-particle batches
+// persistent: one block per SM, blocks pull tiles from a work counter
 int interact_grid_size(int lpp, int n_init, int num_sms) {
     (void)lpp;
-    const int batches = (n_init + 31) / 32;
-    const int blocks_needed = (batches + INTERACT_WARPS - 1) / INTERACT_WARPS;
-    const int cap = num_sms * 16;
-    return blocks_needed < cap ? (blocks_needed > 0 ? blocks_needed : 1) : cap;
+    (void)n_init;
+    return num_sms;
 }
 
 }  // namespace mfree

@@ -10,8 +10,6 @@ constexpr int HASH_BLOCK = 256;
 constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS = 8;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
-constexpr int INTERACT_WARPS = 4;  // warps per block of the pair kernel
-constexpr int QCAP = 128;          // in-support queue per particle before the rescan path
 constexpr int NRES = 20;           // reduced accumulators per particle
 
 // half-step state x + dt/2 * xdot of the predictor (leap_frog.cu:42-70); the
@@ -78,7 +76,8 @@ cudaError_t launch_gather_predict(const StepArgs &a, int blocks, cudaStream_t s)
 __global__ void k_finalize(StepArgs a);
 __global__ void k_force_final(StepArgs a, int num_blocks, float *out);
 
-// launches the pair kernel for the configured variant (mfree_interact.cu)
+// launches the pair kernel for the configured variant (mfree_interact.cu);
+// grid <= 0 only prepares the variant (shared-memory attribute)
 cudaError_t launch_interact(const StepArgs &a, int lanes_per_particle, int grid, cudaStream_t s);
 int interact_grid_size(int lanes_per_particle, int n_init, int num_sms);
 

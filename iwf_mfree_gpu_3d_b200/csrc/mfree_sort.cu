@@ -31,6 +31,7 @@ __global__ void k_clock(StepArgs a, int record_mode) {
     const Params &P = a.p;
     if (c->pending) c->t = c->t + P.dt;  // main(): global_time_current += dt after each iteration
     c->pending = 1;
+    c->tile_next = 0;
     const float t = c->t;
     c->record = record_mode == 1 ? 1
                 : record_mode == 2 ? (P.record_every > 0 && (c->step_index % P.record_every) == 0)
@@ -270,13 +271,14 @@ __global__ void __launch_bounds__(256) k_gather_predict(StepArgs a) {
             artificial_stress(hs.S[0], hs.S[1], hs.S[2], hs.S[3], hs.S[4], hs.S[5], prs, hs.rho, P.stresseps, Rr);
     }
     const float ir2 = 1.0f / (hs.rho * hs.rho);
-    Records r = a.r;
-    r.P[i] = make_float4(hs.x, hs.y, hs.z, fc.w);  // raw tool_particle value
-    r.V[i] = make_float4(hs.vx, hs.vy, hs.vz, hs.rho);
-    r.A[i] = make_float4((hs.S[0] - prs) * ir2, (hs.S[1] - prs) * ir2, (hs.S[2] - prs) * ir2, hs.S[3] * ir2);
-    r.B[i] = make_float4(hs.S[4] * ir2, hs.S[5] * ir2, sqrtf(P.K / hs.rho), pos.w);
-    r.R[i] = make_float4(Rr[0], Rr[1], Rr[2], Rr[3]);
-    r.C[i] = make_float4(Rr[4], Rr[5], hs.T, P.mass / hs.rho);
+    Rec r;
+    r.P = make_float4(hs.x, hs.y, hs.z, fc.w);  // raw tool_particle value
+    r.V = make_float4(hs.vx, hs.vy, hs.vz, hs.rho);
+    r.A = make_float4((hs.S[0] - prs) * ir2, (hs.S[1] - prs) * ir2, (hs.S[2] - prs) * ir2, hs.S[3] * ir2);
+    r.B = make_float4(hs.S[4] * ir2, hs.S[5] * ir2, sqrtf(P.K / hs.rho), pos.w);
+    r.R = make_float4(Rr[0], Rr[1], Rr[2], Rr[3]);
+    r.C = make_float4(Rr[4], Rr[5], hs.T, P.mass / hs.rho);
+    a.r.rec[i] = r;
     if (P.diagnostics) a.s.pos_half[i] = make_float4(hs.x, hs.y, hs.z, 0.f);
 }
 
