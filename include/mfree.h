@@ -113,7 +113,8 @@ typedef struct {
                                    blanked (the reference prints ALARM and writes out of
                                    bounds, grid_gpu_green.cu:56-58)                     */
     int64_t contact_search_cap; /* contact shell searches stopped by the bound          */
-    int64_t nan_blanked;        /* particles kept blanked because a rate is NaN/Inf     */
+    int64_t nan_blanked;        /* blanked particles with a NaN/Inf position or rate,
+                                   summed over steps                                    */
 } mfree_counters;
 
 typedef struct mfree_ctx mfree_ctx;

@@ -15,10 +15,10 @@
 //   The deviatoric stress is symmetric in the reference (every writer keeps
 //   S[c][r] == S[r][c]: predict/correct element-wise, Jaumann
 //   omega*S + S*omega^T, radial return), so 6 components are stored.
-//   half-step neighbour records (one 96-byte record per particle, in sorted
-//   order, written by the predictor and read by the pair loop; a halo column
-//   of records is one contiguous range, staged into shared memory by a single
-//   bulk copy):
+//   half-step neighbour records, six float4 arrays (96 bytes per particle) in
+//   sorted order, written by the predictor and read by the pair loop; a halo
+//   column is one contiguous range of each array, staged into shared memory by
+//   one bulk copy per array:
 //     P = (x, y, z, tool_flag)      V = (vx, vy, vz, rho)
 //     A = sigma(xx, yy, zz, xy)     B = (sigma_xz, sigma_yz, c = sqrt(K/rho), h)
 //     R = R(xx, yy, zz, xy)         C = (R_xz, R_yz, T, m/rho)
@@ -103,13 +103,13 @@ struct State {
     float4 *pos4, *vel4, *sa4, *sb4, *da4, *dv4, *dsa4, *dsb4, *fc4, *ft4, *bc4, *lo4, *lo4b;
 };
 
-struct __align__(16) Rec {
+struct Rec {
     float4 P, V, A, B, R, C;
 };
-static_assert(sizeof(Rec) == 96, "neighbour record must be 96 bytes");
+enum { REC_P = 0, REC_V, REC_A, REC_B, REC_R, REC_C, REC_N };
 
 struct Records {
-    Rec *rec;
+    float4 *f[REC_N];  // one allocation of REC_N * n_init float4, f[k] = base + k * n_init
 };
 
 struct Scratch {

@@ -124,7 +124,7 @@ void invalidate_graphs(mfree_ctx *c) {
     c->graph_valid = false;
 }
 
-int default_lpp() { return 8; }
+int default_lpp() { return 16; }
 
 Params make_params(const mfree_ctx *c) {
     Params P{};
@@ -348,9 +348,14 @@ int enqueue_step(mfree_ctx *c, int record_mode, int record_every, bool timed = f
 }
 
 int copy_records(mfree_ctx *c, std::vector<Rec> &dst) {
-    dst.resize(c->n_init);
-    CUDA_TRY(cudaMemcpyAsync(dst.data(), c->rec.rec, sizeof(Rec) * c->n_init, cudaMemcpyDeviceToHost, c->stream));
+    const int n = c->n_init;
+    std::vector<float4> raw(size_t(REC_N) * n);
+    CUDA_TRY(cudaMemcpyAsync(raw.data(), c->rec.f[0], sizeof(float4) * raw.size(), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    dst.resize(n);
+    for (int i = 0; i < n; i++)
+        dst[i] = Rec{raw[i], raw[size_t(n) + i], raw[2 * size_t(n) + i], raw[3 * size_t(n) + i],
+                     raw[4 * size_t(n) + i], raw[5 * size_t(n) + i]};
     return MFREE_OK;
 }
 
@@ -392,7 +397,11 @@ int mfree_create(int n, const float *pos4, const float *vel4, const float *rho, 
         for (auto p : f)
             if ((st = dalloc(c.get(), p, n, L))) return st;
     }
-    if ((st = dalloc(c.get(), &c->rec.rec, n, L))) return st;
+    {
+        float4 *base = nullptr;
+        if ((st = dalloc(c.get(), &base, size_t(REC_N) * n, L))) return st;
+        for (int k = 0; k < REC_N; k++) c->rec.f[k] = base + size_t(k) * n;
+    }
     if ((st = dalloc(c.get(), &c->scr.key, n, L))) return st;
     if ((st = dalloc(c.get(), &c->scr.key_sorted, n, L))) return st;
     if ((st = dalloc(c.get(), &c->scr.perm, n, L))) return st;
@@ -441,7 +450,7 @@ int mfree_create(int n, const float *pos4, const float *vel4, const float *rho, 
     CUDA_TRY(up(S.bc4, hbc));
     CUDA_TRY(up(S.lo4, hz));
     CUDA_TRY(up(S.lo4b, hz));
-    CUDA_TRY(cudaMemsetAsync(c->rec.rec, 0, sizeof(Rec) * n, c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->rec.f[0], 0, sizeof(float4) * REC_N * n, c->stream));
     CUDA_TRY(cudaMemcpyAsync(c->scr.perm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(cudaMemsetAsync(c->scr.key_sorted, 0, sizeof(int) * n, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));

@@ -118,10 +118,10 @@ __device__ __forceinline__ void pair_body(const Params &P, const IData &I, const
         acc[11] = fmaf(txz, gx, fmaf(tyz, gy, fmaf(tzz, gz, acc[11])));
         const float vr = -(dvx * dx + dvy * dy + dvz * dz);  // (v_i - v_j).(x_i - x_j)
         const float rhoij = 0.5f * (I.rho + Vj.w);
-        const float irho = 1.0f / rhoij;
-        if (vr < 0.f) {
+        const float irho = __fdividef(1.0f, rhoij);
+        {   // artificial viscosity for approaching pairs (vr < 0), without a branch
             const float cij = 0.5f * (I.c + Bj.z), hij = 0.5f * (I.h + Bj.w);
-            const float mu = (hij * vr) / (r2 + P.av_eta * P.av_eta * hij * hij);
+            const float mu = vr < 0.f ? __fdividef(hij * vr, r2 + P.av_eta * P.av_eta * hij * hij) : 0.f;
             const float pij = (-P.av_alpha * cij * mu + P.av_beta * mu * mu) * irho;
             acc[12] = fmaf(-pij, gx, acc[12]);
             acc[13] = fmaf(-pij, gy, acc[13]);
@@ -134,7 +134,7 @@ __device__ __forceinline__ void pair_body(const Params &P, const IData &I, const
     }
     if (COND == MFREE_COND_BROOKSHAW) {
         // 2 (m/rho_j)(T_i - T_j) e.grad W / r = 2 V_j (T_i - T_j) (d.grad W)/r^2; factor 2 in the epilogue
-        acc[18] = fmaf(volj * (I.T - Cj.z), (dx * gx + dy * gy + dz * gz) / r2, acc[18]);
+        acc[18] = fmaf(volj * (I.T - Cj.z), __fdividef(dx * gx + dy * gy + dz * gz, r2), acc[18]);
     }
 }
 
@@ -285,36 +285,38 @@ __device__ void epilogue(const StepArgs &a, int i, const float *res) {
 // ---------------------------------------------------------- pair kernel --
 // Tile = TX x TY x TZ cells of the cell grid; its particles are 16 contiguous
 // column ranges of the sorted order.  Their 5x5x5 stencils lie in the halo of
-// HX x HY x HZ cells, i.e. 64 contiguous column ranges of neighbour records,
-// which one bulk copy each (cp.async.bulk, completion on an mbarrier) stages
-// into shared memory.  A tile whose halo exceeds the staging capacity reads
-// the same records from global memory instead.
+// HX x HY x HZ cells: 64 contiguous column ranges of each record array, which
+// one bulk copy per column and array (cp.async.bulk, completion counted on an
+// mbarrier) stages into six shared-memory arrays.  A tile whose halo exceeds
+// the staging capacity reads the same records from global memory instead.
 constexpr int TX = 4, TY = 4, TZ = 6;
 constexpr int HX = TX + 4, HY = TY + 4, HZ = TZ + 4;
 constexpr int NHC = HX * HY;           // halo columns
 constexpr int NTC = TX * TY;           // target columns
 constexpr int TILE_THREADS = 512;
 constexpr int TILE_WARPS = TILE_THREADS / 32;
-constexpr int TCAP = 256;              // targets per pass of a tile
+constexpr int TCAP = 320;              // targets per pass of a tile
 constexpr int QCAP_T = 96;             // in-support queue per target before the rescan path
 constexpr int SMEM_LIMIT = 232448;     // per-block shared memory of sm_100
 
 template <int LPP> struct TileSmem {
     static constexpr int G = 32 / LPP;
     float res[TCAP][NRES + 1];
+    int tgt[TCAP];       // sorted index of each target of the pass
     int q[TILE_WARPS][G][QCAP_T];
     int cbase[TILE_WARPS][G][25];
     int cpref[TILE_WARPS][G][26];
     int cellstart[NHC][HZ + 1];
-    int hoff[NHC];       // staged offset of halo column
-    int hstart[NHC];     // global start of halo column
+    int hoff[NHC];       // staged offset of a halo column
+    int hstart[NHC];     // global start of a halo column
+    int hlen[NHC];
     int tstart[NTC];
     int tpref[NTC + 1];
     unsigned long long bar;
     int tile, total, staged, parity;
 };
 template <int LPP> __host__ __device__ constexpr int rec_capacity() {
-    return int((SMEM_LIMIT - sizeof(TileSmem<LPP>) - 256) / sizeof(Rec));
+    return int((SMEM_LIMIT - ((sizeof(TileSmem<LPP>) + 127) / 128) * 128) / (REC_N * sizeof(float4)));
 }
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return unsigned(__cvta_generic_to_shared(p)); }
@@ -341,22 +343,211 @@ __device__ __forceinline__ void bulk_to_smem(void *dst, const void *src, unsigne
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// inclusive scan over the LPP lanes of a group
+template <int LPP> __device__ __forceinline__ int group_scan(int v, int sl) {
+#pragma unroll
+    for (int o = 1; o < LPP; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, v, o, LPP);
+        if (sl >= o) v += y;
+    }
+    return v;
+}
+
+// one target: stencil ranges, pass A (support, PSE, queue), CSPM pass over
+// the queue, pair pass over the queue, group reduction
+template <int LPP, bool CSPM, int COND, bool STAGED>
+__device__ __forceinline__ void process_target(const StepArgs &a, TileSmem<LPP> &sm, const float4 *RF, int rstride,
+                                               int i, bool valid, int tt, int warp, int g, int sl, int lane, int X0,
+                                               int Y0, int zl) {
+    const Params &P = a.p;
+    const int nx = P.gnx, ny = P.gny, nz = P.gnz;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const unsigned gmask = LPP == 32 ? 0xffffffffu : (((1u << LPP) - 1u) << (g * LPP));
+    // the six record arrays at RF + k * rstride (shared memory or global)
+    const float4 *__restrict__ rP = RF + REC_P * rstride;
+    const float4 *__restrict__ rV = RF + REC_V * rstride;
+    const float4 *__restrict__ rA = RF + REC_A * rstride;
+    const float4 *__restrict__ rB = RF + REC_B * rstride;
+    const float4 *__restrict__ rR = RF + REC_R * rstride;
+    const float4 *__restrict__ rC = RF + REC_C * rstride;
+    IData I;
+    {
+        const Records &G_ = a.r;
+        const float4 Pi = G_.f[REC_P][i], Vi = G_.f[REC_V][i], Ai = G_.f[REC_A][i], Bi = G_.f[REC_B][i],
+                     Ri = G_.f[REC_R][i], Ci = G_.f[REC_C][i];
+        I.x = Pi.x; I.y = Pi.y; I.z = Pi.z; I.tool = Pi.w;
+        I.vx = Vi.x; I.vy = Vi.y; I.vz = Vi.z; I.rho = Vi.w;
+        I.s[0] = Ai.x; I.s[1] = Ai.y; I.s[2] = Ai.z; I.s[3] = Ai.w; I.s[4] = Bi.x; I.s[5] = Bi.y;
+        I.c = Bi.z; I.h = Bi.w;
+        I.R[0] = Ri.x; I.R[1] = Ri.y; I.R[2] = Ri.z; I.R[3] = Ri.w; I.R[4] = Ci.x; I.R[5] = Ci.y;
+        I.T = Ci.z;
+        I.h1 = 1.0f / I.h;
+        I.fac = 0.31830988618379067f * I.h1 * I.h1 * I.h1;
+    }
+    int *cb = sm.cbase[warp][g];
+    int *cp = sm.cpref[warp][g];
+    int *qq = sm.q[warp][g];
+    // ---- the 25 stencil columns as ranges of the record arrays, with their prefix
+    {
+        const unsigned key = a.s.key_sorted[i];
+        const int nyz = ny * nz;
+        const int gi = int(key) / nyz, rem = int(key) - gi * nyz, gj = rem / nz, gk = rem - gj * nz;
+        const int klo = max(gk - 2, 0) - zl, khi = min(gk + 2, nz - 1) - zl + 1;
+        constexpr int NSET = (25 + LPP - 1) / LPP;
+        int carry = 0;
+#pragma unroll
+        for (int k = 0; k < NSET; k++) {
+            const int c = sl + k * LPP;
+            int b = 0, l = 0;
+            if (valid && c < 25) {
+                const int cx = gi + c / 5 - 2, cy = gj + c % 5 - 2;
+                if (cx >= 0 && cx < nx && cy >= 0 && cy < ny) {
+                    const int lc = (cx - X0 + 2) * HY + (cy - Y0 + 2);
+                    const int s0 = sm.cellstart[lc][klo];
+                    l = sm.cellstart[lc][khi] - s0;
+                    b = STAGED ? sm.hoff[lc] + (s0 - sm.hstart[lc]) : s0;
+                }
+            }
+            const int inc = group_scan<LPP>(l, sl);
+            if (c < 25) {
+                cb[c] = b;
+                cp[c] = carry + inc - l;
+            }
+            carry += __shfl_sync(0xffffffffu, inc, (g * LPP) + LPP - 1);
+        }
+        if (sl == 0) cp[25] = carry;
+    }
+    __syncwarp();
+    const int total = cp[25];
+    int maxtotal = total;
+#pragma unroll
+    for (int o = 16; o >= LPP; o >>= 1) maxtotal = max(maxtotal, __shfl_xor_sync(0xffffffffu, maxtotal, o));
+    // ---- pass A: support test, PSE, queue
+    const float inv_h2 = I.h1 * I.h1;
+    int col = 0, qn = 0, cnt = 0;
+    float pse = 0.f;
+    for (int k0 = 0; k0 < maxtotal; k0 += LPP) {
+        const int k = k0 + sl;
+        bool ins = false;
+        int j = 0;
+        if (k < total) {
+            while (cp[col + 1] <= k) col++;
+            j = cb[col] + (k - cp[col]);
+            const float4 Pj = rP[j];
+            const float dx = I.x - Pj.x, dy = I.y - Pj.y, dz = I.z - Pj.z;
+            const float r2 = dist2_rn(dx, dy, dz);
+            ins = in_support(r2, I.h);
+            if (COND == MFREE_COND_PSE) {
+                const float4 Cj = rC[j];
+                pse = fmaf((Cj.z - I.T) * Cj.w, __expf(-r2 * inv_h2), pse);
+            }
+        }
+        cnt += ins ? 1 : 0;
+        const unsigned m = __ballot_sync(0xffffffffu, ins) & gmask;
+        if (ins) {
+            const int pos = qn + __popc(m & lt_mask);
+            if (pos < QCAP_T) qq[pos] = j;
+        }
+        qn += __popc(m);
+    }
+    __syncwarp();
+    const int qv = min(qn, QCAP_T);
+    int maxq = qv;
+#pragma unroll
+    for (int o = 16; o >= LPP; o >>= 1) maxq = max(maxq, __shfl_xor_sync(0xffffffffu, maxq, o));
+    const bool overflow = __any_sync(0xffffffffu, qn > QCAP_T);
+    // in-support neighbours beyond the queue: found again by rescanning
+    auto for_overflow = [&](auto &&fn) {
+        int col2 = 0, ord = 0;
+        for (int k0 = 0; k0 < maxtotal; k0 += LPP) {
+            const int k = k0 + sl;
+            bool ins = false;
+            int j = 0;
+            if (k < total && qn > QCAP_T) {
+                while (cp[col2 + 1] <= k) col2++;
+                j = cb[col2] + (k - cp[col2]);
+                const float4 Pj = rP[j];
+                ins = in_support(dist2_rn(I.x - Pj.x, I.y - Pj.y, I.z - Pj.z), I.h);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, ins) & gmask;
+            const int pos = ord + __popc(m & lt_mask);
+            if (ins && pos >= QCAP_T) fn(j);
+            ord += __popc(m);
+        }
+    };
+    // ---- CSPM matrix over the in-support neighbours (interactions_gpu.cu:227-295)
+    float invB[9] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};
+    if (CSPM) {
+        float Bm[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) Bm[k] = 0.f;
+        auto bterm = [&](int j) {
+            const float4 Pj = rP[j];
+            if (I.tool == 1.f || Pj.w == 1.f) return;
+            const float dx = I.x - Pj.x, dy = I.y - Pj.y, dz = I.z - Pj.z;
+            float w, dfac;
+            spline(dist2_rn(dx, dy, dz), I.h1, I.fac, w, dfac);
+            const float vol = -rC[j].w;
+            const float d[3] = {dx, dy, dz};
+            const float gr[3] = {dfac * dx, dfac * dy, dfac * dz};
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int r = 0; r < 3; r++) Bm[c * 3 + r] = fmaf(vol * d[r], gr[c], Bm[c * 3 + r]);
+        };
+        for (int q0 = 0; q0 < maxq; q0 += LPP) {
+            const int q = q0 + sl;
+            if (q < qv) bterm(qq[q]);
+        }
+        if (overflow) for_overflow(bterm);
+#pragma unroll
+        for (int o = LPP / 2; o >= 1; o >>= 1)
+#pragma unroll
+            for (int k = 0; k < 9; k++) Bm[k] += __shfl_xor_sync(0xffffffffu, Bm[k], o);
+        const float det = det3(Bm);
+        if (det > 9.99999994e-9f) inv3(Bm, det, invB);
+    }
+    // ---- pair body over the in-support neighbours
+    float acc[19];
+#pragma unroll
+    for (int k = 0; k < 19; k++) acc[k] = 0.f;
+    auto pterm = [&](int j) { pair_body<CSPM, COND>(P, I, invB, rP[j], rV[j], rA[j], rB[j], rR[j], rC[j], acc); };
+    for (int q0 = 0; q0 < maxq; q0 += LPP) {
+        const int q = q0 + sl;
+        if (q < qv) pterm(qq[q]);
+    }
+    if (overflow) for_overflow(pterm);
+    if (COND == MFREE_COND_PSE) acc[18] = pse;
+#pragma unroll
+    for (int o = LPP / 2; o >= 1; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 19; k++) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    }
+    if (sl == 0 && valid) {
+        float *rs = sm.res[tt];
+#pragma unroll
+        for (int k = 0; k < 19; k++) rs[k] = acc[k];
+        rs[19] = __int_as_float(cnt);
+    }
+    __syncwarp();
+}
+
 template <int LPP, bool CSPM, int COND, bool PREC>
 __global__ void __launch_bounds__(TILE_THREADS, 1) k_interact(StepArgs a, int ntx, int nty, int ntz) {
     constexpr int G = 32 / LPP;
     constexpr int CAP = rec_capacity<LPP>();
     extern __shared__ __align__(128) unsigned char dyn[];
     TileSmem<LPP> &sm = *reinterpret_cast<TileSmem<LPP> *>(dyn);
-    Rec *srec = reinterpret_cast<Rec *>(dyn + ((sizeof(TileSmem<LPP>) + 127) / 128) * 128);
+    float4 *sarr = reinterpret_cast<float4 *>(dyn + ((sizeof(TileSmem<LPP>) + 127) / 128) * 128);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane / LPP, sl = lane - g * LPP;
-    const unsigned lt_mask = (1u << lane) - 1u;
-    const unsigned gmask = LPP == 32 ? 0xffffffffu : (((1u << LPP) - 1u) << (g * LPP));
     const Params &P = a.p;
     const int nx = P.gnx, ny = P.gny, nz = P.gnz;
     const int *__restrict__ first = a.s.first;
-    const Rec *__restrict__ grec = a.r.rec;
     const int ntiles = ntx * nty * ntz;
+    const float4 *gbase = a.r.f[0];  // the record arrays are one allocation: f[k] = f[0] + k * n_init
+    const int gstride = P.n_init;
     if (threadIdx.x == 0) {
         mbar_init(&sm.bar, 1);
         sm.parity = 0;
@@ -372,7 +563,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 1) k_interact(StepArgs a, int nt
         const int X0 = tx * TX, Y0 = ty * TY, Z0 = tz * TZ;
         const int zl = max(Z0 - 2, 0), zh = min(Z0 + TZ + 1, nz - 1);
         const int nzr = zh - zl + 2;  // cell starts per halo column (inclusive end)
-        // ---- tables: halo cell starts and target ranges
+        // ---- tables: halo cell starts and target column ranges
         for (int e = threadIdx.x; e < NHC * (HZ + 1); e += TILE_THREADS) {
             const int c = e / (HZ + 1), k = e - c * (HZ + 1);
             const int cx = X0 - 2 + c / HY, cy = Y0 - 2 + c % HY;
@@ -393,41 +584,47 @@ __global__ void __launch_bounds__(TILE_THREADS, 1) k_interact(StepArgs a, int nt
             sm.tpref[c] = len;
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            int acc = 0;
-            for (int c = 0; c < NTC; c++) {
-                const int l = sm.tpref[c];
-                sm.tpref[c] = acc;
-                acc += l;
-            }
-            sm.tpref[NTC] = acc;
-            int tot = 0;
-            for (int c = 0; c < NHC; c++) {
-                sm.hstart[c] = sm.cellstart[c][0];
-                sm.hoff[c] = tot;
+        if (warp == 0) {  // prefix sums of the 64 halo columns and the 16 target columns
+            int len2[2];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int c = lane + 32 * h;
                 const int cx = X0 - 2 + c / HY, cy = Y0 - 2 + c % HY;
-                if (cx >= 0 && cx < nx && cy >= 0 && cy < ny) tot += sm.cellstart[c][nzr - 1] - sm.cellstart[c][0];
+                const bool in = cx >= 0 && cx < nx && cy >= 0 && cy < ny;
+                len2[h] = in ? sm.cellstart[c][nzr - 1] - sm.cellstart[c][0] : 0;
+                sm.hstart[c] = sm.cellstart[c][0];
+                sm.hlen[c] = len2[h];
             }
-            sm.total = tot;
-            sm.staged = (acc > 0 && tot <= CAP) ? 1 : 0;
-            if (sm.staged && tot > 0) mbar_expect(&sm.bar, unsigned(tot) * unsigned(sizeof(Rec)));
+            const int i0 = group_scan<32>(len2[0], lane);
+            const int t0 = __shfl_sync(0xffffffffu, i0, 31);
+            const int i1 = group_scan<32>(len2[1], lane);
+            sm.hoff[lane] = i0 - len2[0];
+            sm.hoff[lane + 32] = t0 + i1 - len2[1];
+            const int tot = t0 + __shfl_sync(0xffffffffu, i1, 31);
+            const int tl = lane < NTC ? sm.tpref[lane] : 0;
+            const int ti = group_scan<32>(tl, lane);
+            __syncwarp();
+            if (lane < NTC) sm.tpref[lane] = ti - tl;
+            const int T = __shfl_sync(0xffffffffu, ti, 31);
+            if (lane == 0) {
+                sm.tpref[NTC] = T;
+                sm.total = tot;
+                sm.staged = (T > 0 && tot <= CAP) ? 1 : 0;
+                if (sm.staged && tot > 0) mbar_expect(&sm.bar, unsigned(tot) * unsigned(REC_N * sizeof(float4)));
+            }
         }
         __syncthreads();
         const int T = sm.tpref[NTC];
         if (T == 0) continue;  // (the loop head synchronises before the next tile)
         const bool staged = sm.staged != 0;
         if (staged && sm.total > 0) {
-            if (threadIdx.x < NHC) {
-                const int c = threadIdx.x;
-                const int cx = X0 - 2 + c / HY, cy = Y0 - 2 + c % HY;
-                if (cx >= 0 && cx < nx && cy >= 0 && cy < ny) {
-                    const int len = sm.cellstart[c][nzr - 1] - sm.cellstart[c][0];
-                    if (len > 0)
-                        bulk_to_smem(srec + sm.hoff[c], grec + sm.hstart[c], unsigned(len) * unsigned(sizeof(Rec)),
-                                     &sm.bar);
-                }
+            if (threadIdx.x < REC_N * NHC) {
+                const int k = threadIdx.x / NHC, c = threadIdx.x - k * NHC;
+                const int len = sm.hlen[c];
+                if (len > 0)
+                    bulk_to_smem(sarr + k * CAP + sm.hoff[c], gbase + size_t(k) * gstride + sm.hstart[c],
+                                 unsigned(len) * unsigned(sizeof(float4)), &sm.bar);
             }
-            // bounded wait for the staged halo
             const unsigned par = unsigned(sm.parity);
             unsigned it = 0;
             bool ok = true;
@@ -448,183 +645,32 @@ __global__ void __launch_bounds__(TILE_THREADS, 1) k_interact(StepArgs a, int nt
             }
             if (threadIdx.x == 0) sm.parity ^= 1;
         }
-        const Rec *R = staged ? srec : grec;
         // ---- targets, TCAP per pass
         for (int t0 = 0; t0 < T; t0 += TCAP) {
             const int tn = min(TCAP, T - t0);
-            const int rounds = (tn + TILE_WARPS * G - 1) / (TILE_WARPS * G);
-#pragma unroll 1
-            for (int rnd = 0; rnd < rounds; rnd++) {
-                const int tt = rnd * TILE_WARPS * G + warp * G + g;  // target slot in this pass
-                const bool valid = tt < tn;
-                int i = 0;
-                {
-                    const int tg = t0 + (valid ? tt : 0);
-                    int c = 0;
-                    while (c < NTC - 1 && sm.tpref[c + 1] <= tg) c++;
-                    i = sm.tstart[c] + (tg - sm.tpref[c]);
-                }
-                const Rec &Ri = grec[i];
-                IData I;
-                {
-                    const float4 Pi = Ri.P, Vi = Ri.V, Ai = Ri.A, Bi = Ri.B, RRi = Ri.R, Ci = Ri.C;
-                    I.x = Pi.x; I.y = Pi.y; I.z = Pi.z; I.tool = Pi.w;
-                    I.vx = Vi.x; I.vy = Vi.y; I.vz = Vi.z; I.rho = Vi.w;
-                    I.s[0] = Ai.x; I.s[1] = Ai.y; I.s[2] = Ai.z; I.s[3] = Ai.w; I.s[4] = Bi.x; I.s[5] = Bi.y;
-                    I.c = Bi.z; I.h = Bi.w;
-                    I.R[0] = RRi.x; I.R[1] = RRi.y; I.R[2] = RRi.z; I.R[3] = RRi.w; I.R[4] = Ci.x; I.R[5] = Ci.y;
-                    I.T = Ci.z;
-                    I.h1 = 1.0f / I.h;
-                    I.fac = 0.31830988618379067f * I.h1 * I.h1 * I.h1;
-                }
-                // stencil columns of this target as ranges of R
-                {
-                    const unsigned key = a.s.key_sorted[i];
-                    const int nyz = ny * nz;
-                    const int gi = int(key) / nyz, rem = int(key) - gi * nyz, gj = rem / nz, gk = rem - gj * nz;
-                    const int klo = max(gk - 2, 0) - zl, khi = min(gk + 2, nz - 1) - zl + 1;
-                    for (int c = sl; c < 25; c += LPP) {
-                        const int cx = gi + c / 5 - 2, cy = gj + c % 5 - 2;
-                        int b = 0, l = 0;
-                        if (valid && cx >= 0 && cx < nx && cy >= 0 && cy < ny) {
-                            const int lc = (cx - X0 + 2) * HY + (cy - Y0 + 2);
-                            const int s0 = sm.cellstart[lc][klo];
-                            l = sm.cellstart[lc][khi] - s0;
-                            b = staged ? sm.hoff[lc] + (s0 - sm.hstart[lc]) : s0;
-                        }
-                        sm.cbase[warp][g][c] = b;
-                        sm.cpref[warp][g][c] = l;
-                    }
-                }
-                __syncwarp();
-                if (sl == 0) {
-                    int acc = 0;
-                    for (int c = 0; c < 25; c++) {
-                        const int l = sm.cpref[warp][g][c];
-                        sm.cpref[warp][g][c] = acc;
-                        acc += l;
-                    }
-                    sm.cpref[warp][g][25] = acc;
-                }
-                __syncwarp();
-                const int total = sm.cpref[warp][g][25];
-                int maxtotal = total;
-#pragma unroll
-                for (int o = 16; o >= LPP; o >>= 1)
-                    maxtotal = max(maxtotal, __shfl_xor_sync(0xffffffffu, maxtotal, o));
-                const int *cb = sm.cbase[warp][g];
-                const int *cp = sm.cpref[warp][g];
-                int *qq = sm.q[warp][g];
-                // ---- pass A: support test, PSE, CSPM matrix, queue
-                const float inv_h2 = I.h1 * I.h1;
-                int col = 0, qn = 0, cnt = 0;
-                float pse = 0.f;
-                float Bm[9];
-#pragma unroll
-                for (int k = 0; k < 9; k++) Bm[k] = 0.f;
-                for (int k0 = 0; k0 < maxtotal; k0 += LPP) {
-                    const int k = k0 + sl;
-                    bool ins = false;
-                    int j = 0;
-                    if (k < total) {
-                        while (cp[col + 1] <= k) col++;
-                        j = cb[col] + (k - cp[col]);
-                        const float4 Pj = R[j].P;
-                        const float dx = I.x - Pj.x, dy = I.y - Pj.y, dz = I.z - Pj.z;
-                        const float r2 = dist2_rn(dx, dy, dz);
-                        ins = in_support(r2, I.h);
-                        if (COND == MFREE_COND_PSE || CSPM) {
-                            const float4 Cj = R[j].C;
-                            if (COND == MFREE_COND_PSE) pse = fmaf((Cj.z - I.T) * Cj.w, __expf(-r2 * inv_h2), pse);
-                            if (CSPM && ins && !(I.tool == 1.f) && !(Pj.w == 1.f)) {
-                                float w, dfac;
-                                spline(r2, I.h1, I.fac, w, dfac);
-                                const float d[3] = {dx, dy, dz};
-                                const float gr[3] = {dfac * dx, dfac * dy, dfac * dz};
-#pragma unroll
-                                for (int c = 0; c < 3; c++)
-#pragma unroll
-                                    for (int r = 0; r < 3; r++) Bm[c * 3 + r] = fmaf(-Cj.w * d[r], gr[c], Bm[c * 3 + r]);
-                            }
-                        }
-                    }
-                    cnt += ins ? 1 : 0;
-                    const unsigned m = __ballot_sync(0xffffffffu, ins) & gmask;
-                    if (ins) {
-                        const int pos = qn + __popc(m & lt_mask);
-                        if (pos < QCAP_T) qq[pos] = j;
-                    }
-                    qn += __popc(m);
-                }
-                __syncwarp();
-                float invB[9] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};
-                if (CSPM) {
-#pragma unroll
-                    for (int o = LPP / 2; o >= 1; o >>= 1)
-#pragma unroll
-                        for (int k = 0; k < 9; k++) Bm[k] += __shfl_xor_sync(0xffffffffu, Bm[k], o);
-                    const float det = det3(Bm);
-                    if (det > 9.99999994e-9f) inv3(Bm, det, invB);
-                }
-                // ---- pass B: pair body on the in-support queue
-                float acc[19];
-#pragma unroll
-                for (int k = 0; k < 19; k++) acc[k] = 0.f;
-                const int qv = min(qn, QCAP_T);
-                int maxq = qv;
-#pragma unroll
-                for (int o = 16; o >= LPP; o >>= 1) maxq = max(maxq, __shfl_xor_sync(0xffffffffu, maxq, o));
-                for (int q0 = 0; q0 < maxq; q0 += LPP) {
-                    const int q = q0 + sl;
-                    if (q < qv) {
-                        const Rec &Rj = R[qq[q]];
-                        pair_body<CSPM, COND>(P, I, invB, Rj.P, Rj.V, Rj.A, Rj.B, Rj.R, Rj.C, acc);
-                    }
-                }
-                if (__any_sync(0xffffffffu, qn > QCAP_T)) {
-                    int col2 = 0, ord = 0;
-                    for (int k0 = 0; k0 < maxtotal; k0 += LPP) {
-                        const int k = k0 + sl;
-                        bool ins = false;
-                        int j = 0;
-                        if (k < total && qn > QCAP_T) {
-                            while (cp[col2 + 1] <= k) col2++;
-                            j = cb[col2] + (k - cp[col2]);
-                            const float4 Pj = R[j].P;
-                            ins = in_support(dist2_rn(I.x - Pj.x, I.y - Pj.y, I.z - Pj.z), I.h);
-                        }
-                        const unsigned m = __ballot_sync(0xffffffffu, ins) & gmask;
-                        const int pos = ord + __popc(m & lt_mask);
-                        if (ins && pos >= QCAP_T) {
-                            const Rec &Rj = R[j];
-                            pair_body<CSPM, COND>(P, I, invB, Rj.P, Rj.V, Rj.A, Rj.B, Rj.R, Rj.C, acc);
-                        }
-                        ord += __popc(m);
-                    }
-                }
-                if (COND == MFREE_COND_PSE) acc[18] = pse;
-#pragma unroll
-                for (int o = LPP / 2; o >= 1; o >>= 1) {
-#pragma unroll
-                    for (int k = 0; k < 19; k++) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
-                    cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-                }
-                if (sl == 0 && valid) {
-                    float *rs = sm.res[tt];
-#pragma unroll
-                    for (int k = 0; k < 19; k++) rs[k] = acc[k];
-                    rs[19] = __int_as_float(cnt);
-                }
-                __syncwarp();
-            }
-            __syncthreads();
-            // ---- per-particle rest of the step, one thread per target
             for (int tt = threadIdx.x; tt < tn; tt += TILE_THREADS) {
                 const int tg = t0 + tt;
                 int c = 0;
                 while (c < NTC - 1 && sm.tpref[c + 1] <= tg) c++;
-                epilogue<PREC, COND>(a, sm.tstart[c] + (tg - sm.tpref[c]), sm.res[tt]);
+                sm.tgt[tt] = sm.tstart[c] + (tg - sm.tpref[c]);
             }
+            __syncthreads();
+            const int rounds = (tn + TILE_WARPS * G - 1) / (TILE_WARPS * G);
+#pragma unroll 1
+            for (int rnd = 0; rnd < rounds; rnd++) {
+                const int tt = rnd * TILE_WARPS * G + warp * G + g;
+                const bool valid = tt < tn;
+                const int i = sm.tgt[valid ? tt : 0];
+                if (staged)
+                    process_target<LPP, CSPM, COND, true>(a, sm, sarr, CAP, i, valid, tt, warp, g, sl, lane, X0, Y0,
+                                                          zl);
+                else
+                    process_target<LPP, CSPM, COND, false>(a, sm, gbase, gstride, i, valid, tt, warp, g, sl, lane,
+                                                           X0, Y0, zl);
+            }
+            __syncthreads();
+            // ---- per-particle rest of the step, one thread per target
+            for (int tt = threadIdx.x; tt < tn; tt += TILE_THREADS) epilogue<PREC, COND>(a, sm.tgt[tt], sm.res[tt]);
             __syncthreads();
         }
         fence_proxy_async();  // generic reads of the staged halo precede the next tile's bulk writes

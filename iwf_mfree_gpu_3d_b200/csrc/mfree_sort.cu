@@ -77,7 +77,15 @@ __global__ void __launch_bounds__(HASH_BLOCK) k_hash(StepArgs a) {
                            nan_or_inf(dsa.z) || nan_or_inf(dsa.w) || nan_or_inf(dsb.y) || nan_or_inf(dsb.x) ||
                            nan_or_inf(da.w) || nan_or_inf(dv.w);
                 if (!bad) blanked = 0.f;
-                else if (blanked == 1.f) atomicAdd(&a.clk->nan_blanked, 1ull);
+            }
+            if (blanked == 1.f) {  // count blanked particles carrying a NaN/Inf position or rate
+                float4 da = a.a.da4[i], dv = a.a.dv4[i], dsa = a.a.dsa4[i], dsb = a.a.dsb4[i];
+                bool bad = nan_or_inf(p.x) || nan_or_inf(p.y) || nan_or_inf(p.z) || nan_or_inf(da.x) ||
+                           nan_or_inf(da.y) || nan_or_inf(da.z) || nan_or_inf(dv.x) || nan_or_inf(dv.y) ||
+                           nan_or_inf(dv.z) || nan_or_inf(dsa.x) || nan_or_inf(dsa.y) || nan_or_inf(dsa.z) ||
+                           nan_or_inf(dsa.w) || nan_or_inf(dsb.x) || nan_or_inf(dsb.y) || nan_or_inf(da.w) ||
+                           nan_or_inf(dv.w);
+                if (bad) atomicAdd(&a.clk->nan_blanked, 1ull);
             }
         }
         unsigned key = unsigned(P.num_cell);
@@ -271,14 +279,13 @@ __global__ void __launch_bounds__(256) k_gather_predict(StepArgs a) {
             artificial_stress(hs.S[0], hs.S[1], hs.S[2], hs.S[3], hs.S[4], hs.S[5], prs, hs.rho, P.stresseps, Rr);
     }
     const float ir2 = 1.0f / (hs.rho * hs.rho);
-    Rec r;
-    r.P = make_float4(hs.x, hs.y, hs.z, fc.w);  // raw tool_particle value
-    r.V = make_float4(hs.vx, hs.vy, hs.vz, hs.rho);
-    r.A = make_float4((hs.S[0] - prs) * ir2, (hs.S[1] - prs) * ir2, (hs.S[2] - prs) * ir2, hs.S[3] * ir2);
-    r.B = make_float4(hs.S[4] * ir2, hs.S[5] * ir2, sqrtf(P.K / hs.rho), pos.w);
-    r.R = make_float4(Rr[0], Rr[1], Rr[2], Rr[3]);
-    r.C = make_float4(Rr[4], Rr[5], hs.T, P.mass / hs.rho);
-    a.r.rec[i] = r;
+    const Records &r = a.r;
+    r.f[REC_P][i] = make_float4(hs.x, hs.y, hs.z, fc.w);  // raw tool_particle value
+    r.f[REC_V][i] = make_float4(hs.vx, hs.vy, hs.vz, hs.rho);
+    r.f[REC_A][i] = make_float4((hs.S[0] - prs) * ir2, (hs.S[1] - prs) * ir2, (hs.S[2] - prs) * ir2, hs.S[3] * ir2);
+    r.f[REC_B][i] = make_float4(hs.S[4] * ir2, hs.S[5] * ir2, sqrtf(P.K / hs.rho), pos.w);
+    r.f[REC_R][i] = make_float4(Rr[0], Rr[1], Rr[2], Rr[3]);
+    r.f[REC_C][i] = make_float4(Rr[4], Rr[5], hs.T, P.mass / hs.rho);
     if (P.diagnostics) a.s.pos_half[i] = make_float4(hs.x, hs.y, hs.z, 0.f);
 }
 
