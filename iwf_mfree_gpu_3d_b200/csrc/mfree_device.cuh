@@ -74,6 +74,7 @@ struct Params {
     float mass, K, G, rho0, c0sq;  // c0sq = sqrtf(K/rho0)^2 as do_material_eos computes it
     // correctors (corr_constants)
     float wdeltap, stresseps, xspheps, av_alpha, av_beta, av_eta;
+    float inv_wdeltap;  // 1 / wdeltap (0 when artificial stress is off)
     // thermal
     float wp_alpha, wp_cp, wp_tq, wp_Tinit, wp_eta, tool_alpha;
     int thermal;       // m_thermal of actions_gpu.cu: workpiece or tool diffusivity != 0

@@ -124,7 +124,7 @@ void invalidate_graphs(mfree_ctx *c) {
     c->graph_valid = false;
 }
 
-int default_lpp() { return 16; }
+int default_lpp() { return 8; }
 
 Params make_params(const mfree_ctx *c) {
     Params P{};
@@ -137,6 +137,7 @@ Params make_params(const mfree_ctx *c) {
         P.c0sq = c0 * c0;
     }
     P.wdeltap = c->corr.wdeltap;
+    P.inv_wdeltap = c->corr.wdeltap > 0.f ? 1.0f / c->corr.wdeltap : 0.f;
     P.stresseps = c->corr.stresseps;
     P.xspheps = c->corr.xspheps;
     P.av_alpha = c->corr.alpha;

@@ -101,7 +101,7 @@ __device__ __forceinline__ void pair_body(const Params &P, const IData &I, const
         acc[6] = fmaf(az, gx, acc[6]); acc[7] = fmaf(az, gy, acc[7]); acc[8] = fmaf(az, gz, acc[8]);
         float Rxx = 0.f, Ryy = 0.f, Rzz = 0.f, Rxy = 0.f, Rxz = 0.f, Ryz = 0.f;
         if (P.wdeltap > 0.f) {
-            float fab = w / P.wdeltap;
+            float fab = w * P.inv_wdeltap;
             fab *= fab;
             fab *= fab;
             Rxx = fab * (I.R[0] + Rj.x);
@@ -355,8 +355,8 @@ template <int LPP> __device__ __forceinline__ int group_scan(int v, int sl) {
 
 // one target: stencil ranges, pass A (support, PSE, queue), CSPM pass over
 // the queue, pair pass over the queue, group reduction
-template <int LPP, bool CSPM, int COND, bool STAGED>
-__device__ __forceinline__ void process_target(const StepArgs &a, TileSmem<LPP> &sm, const float4 *RF, int rstride,
+template <int LPP, bool CSPM, int COND, bool STAGED, class SM>
+__device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const float4 *RF, int rstride,
                                                int i, bool valid, int tt, int warp, int g, int sl, int lane, int X0,
                                                int Y0, int zl) {
     const Params &P = a.p;
@@ -423,7 +423,8 @@ __device__ __forceinline__ void process_target(const StepArgs &a, TileSmem<LPP> 
 #pragma unroll
     for (int o = 16; o >= LPP; o >>= 1) maxtotal = max(maxtotal, __shfl_xor_sync(0xffffffffu, maxtotal, o));
     // ---- pass A: support test, PSE, queue
-    const float inv_h2 = I.h1 * I.h1;
+    const float pse_k = -1.44269504088896341f * I.h1 * I.h1;  // exp(-r^2/h^2) = 2^(pse_k r^2)
+    const float four_h2 = __fmul_rn(__fmul_rn(4.0f, I.h), I.h);
     int col = 0, qn = 0, cnt = 0;
     float pse = 0.f;
     for (int k0 = 0; k0 < maxtotal; k0 += LPP) {
@@ -436,10 +437,10 @@ __device__ __forceinline__ void process_target(const StepArgs &a, TileSmem<LPP> 
             const float4 Pj = rP[j];
             const float dx = I.x - Pj.x, dy = I.y - Pj.y, dz = I.z - Pj.z;
             const float r2 = dist2_rn(dx, dy, dz);
-            ins = in_support(r2, I.h);
+            ins = !(r2 >= four_h2) && (r2 > 9.99999994e-9f);  // in_support()
             if (COND == MFREE_COND_PSE) {
                 const float4 Cj = rC[j];
-                pse = fmaf((Cj.z - I.T) * Cj.w, __expf(-r2 * inv_h2), pse);
+                pse = fmaf((Cj.z - I.T) * Cj.w, exp2f(pse_k * r2), pse);
             }
         }
         cnt += ins ? 1 : 0;
@@ -655,18 +656,47 @@ __global__ void __launch_bounds__(TILE_THREADS, 1) k_interact(StepArgs a, int nt
                 sm.tgt[tt] = sm.tstart[c] + (tg - sm.tpref[c]);
             }
             __syncthreads();
-            const int rounds = (tn + TILE_WARPS * G - 1) / (TILE_WARPS * G);
+            // rounds of TILE_WARPS * G targets; a last round with few targets
+            // left uses more lanes per target so fewer warps idle at the barrier
+            int done = 0;
 #pragma unroll 1
-            for (int rnd = 0; rnd < rounds; rnd++) {
-                const int tt = rnd * TILE_WARPS * G + warp * G + g;
-                const bool valid = tt < tn;
-                const int i = sm.tgt[valid ? tt : 0];
-                if (staged)
-                    process_target<LPP, CSPM, COND, true>(a, sm, sarr, CAP, i, valid, tt, warp, g, sl, lane, X0, Y0,
-                                                          zl);
-                else
-                    process_target<LPP, CSPM, COND, false>(a, sm, gbase, gstride, i, valid, tt, warp, g, sl, lane,
-                                                           X0, Y0, zl);
+            while (done < tn) {
+                const int rem = tn - done;
+                if (LPP < 32 && rem <= TILE_WARPS) {
+                    const int tt = done + warp;
+                    const bool valid = tt < tn;
+                    const int i = sm.tgt[valid ? tt : 0];
+                    if (staged)
+                        process_target<32, CSPM, COND, true>(a, sm, sarr, CAP, i, valid, tt, warp, 0, lane, lane, X0,
+                                                             Y0, zl);
+                    else
+                        process_target<32, CSPM, COND, false>(a, sm, gbase, gstride, i, valid, tt, warp, 0, lane, lane,
+                                                              X0, Y0, zl);
+                    done += TILE_WARPS;
+                } else if (LPP < 16 && rem <= 2 * TILE_WARPS) {
+                    const int g2 = lane >> 4, sl2 = lane & 15;
+                    const int tt = done + warp * 2 + g2;
+                    const bool valid = tt < tn;
+                    const int i = sm.tgt[valid ? tt : 0];
+                    if (staged)
+                        process_target<16, CSPM, COND, true>(a, sm, sarr, CAP, i, valid, tt, warp, g2, sl2, lane, X0,
+                                                             Y0, zl);
+                    else
+                        process_target<16, CSPM, COND, false>(a, sm, gbase, gstride, i, valid, tt, warp, g2, sl2, lane,
+                                                              X0, Y0, zl);
+                    done += 2 * TILE_WARPS;
+                } else {
+                    const int tt = done + warp * G + g;
+                    const bool valid = tt < tn;
+                    const int i = sm.tgt[valid ? tt : 0];
+                    if (staged)
+                        process_target<LPP, CSPM, COND, true>(a, sm, sarr, CAP, i, valid, tt, warp, g, sl, lane, X0,
+                                                              Y0, zl);
+                    else
+                        process_target<LPP, CSPM, COND, false>(a, sm, gbase, gstride, i, valid, tt, warp, g, sl, lane,
+                                                               X0, Y0, zl);
+                    done += TILE_WARPS * G;
+                }
             }
             __syncthreads();
             // ---- per-particle rest of the step, one thread per target
