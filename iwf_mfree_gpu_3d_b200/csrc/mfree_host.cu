@@ -92,6 +92,12 @@ struct mfree_ctx {
     double kernel_ms[MFREE_NUM_KERNELS] = {0};
     int kernel_n[MFREE_NUM_KERNELS] = {0};
     cudaEvent_t timer[2] = {nullptr, nullptr};
+    // active count of the last step, copied back asynchronously: a step that
+    // left no particle makes the next call return MFREE_ERR_EMPTY (the
+    // reference exits there, grid_gpu_base.cu:159-163)
+    int *h_nact = nullptr;
+    cudaEvent_t nact_ev = nullptr;
+    bool nact_pending = false;
     // graphs, one per state parity
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int graph_record_every = -1;
@@ -476,6 +482,8 @@ int mfree_destroy(mfree_ctx *c) {
     for (auto e : c->event_pool) cudaEventDestroy(e);
     for (auto e : c->timer)
         if (e) cudaEventDestroy(e);
+    if (c->h_nact) cudaFreeHost(c->h_nact);
+    if (c->nact_ev) cudaEventDestroy(c->nact_ev);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
     return MFREE_OK;
@@ -677,11 +685,33 @@ int mfree_get_tool_cells(mfree_ctx *c, int k, int *cells, int *boxed_src) {
     return MFREE_OK;
 }
 
+static int check_empty(mfree_ctx *c, bool wait) {
+    if (!c->nact_pending) return MFREE_OK;
+    if (!wait && cudaEventQuery(c->nact_ev) != cudaSuccess) return MFREE_OK;
+    CUDA_TRY(cudaEventSynchronize(c->nact_ev));
+    c->nact_pending = false;
+    if (*c->h_nact == 0) return fail(MFREE_ERR_EMPTY, "all particles are blanked (outside the blanking box)");
+    return MFREE_OK;
+}
+
+static int note_active_count(mfree_ctx *c) {
+    if (!c->h_nact) {
+        CUDA_TRY(cudaMallocHost(&c->h_nact, sizeof(int)));
+        CUDA_TRY(cudaEventCreateWithFlags(&c->nact_ev, cudaEventDisableTiming));
+    }
+    CUDA_TRY(cudaMemcpyAsync(c->h_nact, &c->d_clk->n_active, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaEventRecord(c->nact_ev, c->stream));
+    c->nact_pending = true;
+    return MFREE_OK;
+}
+
 int mfree_step(mfree_ctx *c, int record_forces) {
     if (!c) return fail(MFREE_ERR_ARG, "null context");
     int st = ready(c);
     if (st) return st;
+    if ((st = check_empty(c, false))) return st;
     if ((st = enqueue_step(c, record_forces ? 1 : 0, 0, c->timing))) return st;
+    if ((st = note_active_count(c))) return st;
     c->cur ^= 1;
     if (c->pending) c->t = c->t + c->dt;
     c->pending = true;
@@ -693,6 +723,7 @@ int mfree_advance(mfree_ctx *c, int nsteps, int record_every, int use_graph) {
     if (!c || nsteps < 0) return fail(MFREE_ERR_ARG, "bad arguments");
     int st = ready(c);
     if (st) return st;
+    if ((st = check_empty(c, false))) return st;
     if (!use_graph) {
         for (int k = 0; k < nsteps; k++) {
             const bool rec = record_every > 0 && (c->steps % record_every) == 0;
@@ -733,7 +764,7 @@ int mfree_advance(mfree_ctx *c, int nsteps, int record_every, int use_graph) {
         c->pending = true;
         c->steps++;
     }
-    return MFREE_OK;
+    return note_active_count(c);
 }
 
 int mfree_set_kernel_timing(mfree_ctx *c, int on) {
@@ -799,7 +830,7 @@ int mfree_probe_fp32_peak(double *tflops) {
 int mfree_sync(mfree_ctx *c) {
     if (!c) return fail(MFREE_ERR_ARG, "null context");
     CUDA_TRY(cudaStreamSynchronize(c->stream));
-    return MFREE_OK;
+    return check_empty(c, true);
 }
 
 int mfree_get_counts(const mfree_ctx *c, int *n_active, int *n_init) {

@@ -564,7 +564,26 @@ __global__ void __launch_bounds__(TILE_THREADS, 1) k_interact(StepArgs a, int nt
         const int X0 = tx * TX, Y0 = ty * TY, Z0 = tz * TZ;
         const int zl = max(Z0 - 2, 0), zh = min(Z0 + TZ + 1, nz - 1);
         const int nzr = zh - zl + 2;  // cell starts per halo column (inclusive end)
-        // ---- tables: halo cell starts and target column ranges
+        // ---- target column ranges first: empty tiles end here
+        if (threadIdx.x < 32) {
+            const int c = threadIdx.x;
+            int s0 = 0, len = 0;
+            if (c < NTC) {
+                const int cx = X0 + c / TY, cy = Y0 + c % TY;
+                if (cx < nx && cy < ny && Z0 < nz) {
+                    const int cb = (cx * ny + cy) * nz;
+                    s0 = first[cb + Z0];
+                    len = first[cb + min(Z0 + TZ - 1, nz - 1) + 1] - s0;
+                }
+                sm.tstart[c] = s0;
+            }
+            const int ti = group_scan<32>(len, c);
+            if (c < NTC) sm.tpref[c] = ti - len;
+            if (c == 31) sm.tpref[NTC] = ti;
+        }
+        __syncthreads();
+        if (sm.tpref[NTC] == 0) continue;  // (the loop head synchronises before the next tile)
+        // ---- halo cell starts
         for (int e = threadIdx.x; e < NHC * (HZ + 1); e += TILE_THREADS) {
             const int c = e / (HZ + 1), k = e - c * (HZ + 1);
             const int cx = X0 - 2 + c / HY, cy = Y0 - 2 + c % HY;
@@ -572,20 +591,8 @@ __global__ void __launch_bounds__(TILE_THREADS, 1) k_interact(StepArgs a, int nt
             if (k < nzr && cx >= 0 && cx < nx && cy >= 0 && cy < ny) v = first[(cx * ny + cy) * nz + zl + k];
             sm.cellstart[c][k] = v;
         }
-        if (threadIdx.x < NTC) {
-            const int c = threadIdx.x;
-            const int cx = X0 + c / TY, cy = Y0 + c % TY;
-            int s0 = 0, len = 0;
-            if (cx < nx && cy < ny && Z0 < nz) {
-                const int cb = (cx * ny + cy) * nz;
-                s0 = first[cb + Z0];
-                len = first[cb + min(Z0 + TZ - 1, nz - 1) + 1] - s0;
-            }
-            sm.tstart[c] = s0;
-            sm.tpref[c] = len;
-        }
         __syncthreads();
-        if (warp == 0) {  // prefix sums of the 64 halo columns and the 16 target columns
+        if (warp == 0) {  // prefix sum of the 64 halo columns; staging decision
             int len2[2];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
@@ -602,21 +609,14 @@ __global__ void __launch_bounds__(TILE_THREADS, 1) k_interact(StepArgs a, int nt
             sm.hoff[lane] = i0 - len2[0];
             sm.hoff[lane + 32] = t0 + i1 - len2[1];
             const int tot = t0 + __shfl_sync(0xffffffffu, i1, 31);
-            const int tl = lane < NTC ? sm.tpref[lane] : 0;
-            const int ti = group_scan<32>(tl, lane);
-            __syncwarp();
-            if (lane < NTC) sm.tpref[lane] = ti - tl;
-            const int T = __shfl_sync(0xffffffffu, ti, 31);
             if (lane == 0) {
-                sm.tpref[NTC] = T;
                 sm.total = tot;
-                sm.staged = (T > 0 && tot <= CAP) ? 1 : 0;
+                sm.staged = tot <= CAP ? 1 : 0;
                 if (sm.staged && tot > 0) mbar_expect(&sm.bar, unsigned(tot) * unsigned(REC_N * sizeof(float4)));
             }
         }
         __syncthreads();
         const int T = sm.tpref[NTC];
-        if (T == 0) continue;  // (the loop head synchronises before the next tile)
         const bool staged = sm.staged != 0;
         if (staged && sm.total > 0) {
             if (threadIdx.x < REC_N * NHC) {

@@ -135,6 +135,20 @@ def test_velocity_blanking_moves_particle_to_tail():
     sim.close()
 
 
+def test_all_particles_leaving_the_box_is_reported():
+    """The reference prints and exits when every particle has left the box
+    (grid_gpu_base.cu:159-163); here the next call returns MFREE_ERR_EMPTY."""
+    sc = scenes.orthogonal_cutting(10, 6, 5)
+    sim = api.Simulation.from_scene(sc)
+    sim.set_blanking(sc.blank_bbmin, sc.blank_bbmax, sc.blank_vmax, bbvel=np.array([100.0, 0, 0], np.float32))
+    with pytest.raises(api.MfreeError) as e:
+        for _ in range(5):
+            sim.step()
+        sim.sync()
+    assert e.value.status == -6
+    sim.close()
+
+
 def test_secant_iteration_limit_is_reported():
     """With the iteration limit at 1 the radial return reports failures
     through the counters instead of printing (actions_gpu.cu:415-418)."""
@@ -167,7 +181,7 @@ def test_moving_grid_and_blanking_box():
     sc = scenes.small_scene()
     sim = api.Simulation.from_scene(sc)
     orc = oracle.Oracle(sc, prec=64)
-    v = np.array([8.0, 0.0, 0.0], np.float32)  # the box's -x face sweeps past ~40 % of the block in 20 steps
+    v = np.array([3.8, 0.0, 0.0], np.float32)  # the box's -x face sweeps past ~40 % of the block in 20 steps
     sim.set_grid_velocity(v)
     sim.set_blanking(sc.blank_bbmin, sc.blank_bbmax, sc.blank_vmax, bbvel=v)
     import ctypes as C
