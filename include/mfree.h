@@ -240,6 +240,35 @@ int mfree_timer_stop(mfree_ctx *ctx, double *ms);
  * (one process per GPU) */
 int mfree_set_device(int device);
 
+/* ---- cell-list build without allocation -----------------------------------
+ * No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory while they run (a host whose device memory is
+ * reserved up front by its own allocator, or code that cannot afford the
+ * device synchronisation a cudaMalloc may cause).  It computes what the
+ * step's cell-list build computes -- the cell id (int)((x - bbmin)/dx) of each
+ * position, the stable sort by cell id and the cell ranges -- with its
+ * scratch in a fixed-size __device__ array of the library instead of
+ * allocated buffers, and calls no allocation routine.
+ *   pos4:       device pointer, n float4 positions (w ignored)
+ *   bbmin, dx, nx, ny, nz: the grid (mfree_get_grid)
+ *   perm:       device pointer, n ints out: sorted position -> input index;
+ *               positions outside the grid come last, in input order
+ *   cell_first: device pointer, nx*ny*nz + 1 ints out: index of the first
+ *               sorted position of each cell; cell_first[nx*ny*nz] = number of
+ *               positions inside the grid
+ *   stream:     cudaStream_t, or NULL for the legacy default stream
+ * Limits: n <= MFREE_STATIC_MAX_PARTICLES and nx*ny*nz <= MFREE_STATIC_MAX_CELLS,
+ * else MFREE_ERR_ARG.  The array (about 3 MiB) is held on every GPU that loads
+ * the library until the process exits.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls share the array and it keeps the last
+ * call's contents (the counters are cleared at the start of each call): calls
+ * that overlap on the GPU race. */
+#define MFREE_STATIC_MAX_PARTICLES 262144
+#define MFREE_STATIC_MAX_CELLS     524288
+int mfree_cell_list_static(const float *pos4, int n, const float bbmin[3], float dx, int nx, int ny, int nz,
+                           int *perm, int *cell_first, void *stream);
+
 /* ---- scene files (the reference's setup readers) ------------------------- */
 /* json_read_triangles (json_reader.cpp:108-117): MeshLab JSON */
 int mfree_read_mesh_json(const char *path, float **verts, int *nv, int **tris, int *nt);

@@ -39,6 +39,7 @@ EXPORTS = [
     "mfree_get_field_f64", "mfree_get_cells", "mfree_get_grid", "mfree_get_counters", "mfree_read_mesh_json",
     "mfree_read_mesh_ldynak", "mfree_free", "mfree_set_kernel_timing", "mfree_get_kernel_times",
     "mfree_probe_fp32_peak", "mfree_timer_start", "mfree_timer_stop", "mfree_set_device",
+    "mfree_cell_list_static",
 ]
 KERNELS = ["clock", "hash", "scan_reduce", "scan_top", "scan_down", "scatter", "cell_fixup", "gather_predict",
            "interact", "finalize", "force_final"]
@@ -131,6 +132,7 @@ def lib(path: str = LIB_PATH):
     L.mfree_timer_start.argtypes = [P]
     L.mfree_timer_stop.argtypes = [P, C.POINTER(C.c_double)]
     L.mfree_set_device.argtypes = [I]
+    L.mfree_cell_list_static.argtypes = [P, I, fp, F, I, I, I, P, P, P]
     _lib = L
     return L
 

@@ -32,6 +32,12 @@ int fail(int code, const std::string &msg) {
     return code;
 }
 
+}  // namespace
+
+void mfree::set_last_error(const std::string &msg) { g_err = msg; }
+
+namespace {
+
 #define CUDA_TRY(x)                                                                        \
     do {                                                                                   \
         cudaError_t e_ = (x);                                                              \

@@ -2,6 +2,8 @@
 // translation units.
 #pragma once
 
+#include <string>
+
 #include "mfree_device.cuh"
 
 namespace mfree {
@@ -80,6 +82,9 @@ __global__ void k_force_final(StepArgs a, int num_blocks, float *out);
 // grid <= 0 only prepares the variant (shared-memory attribute)
 cudaError_t launch_interact(const StepArgs &a, int lanes_per_particle, int grid, cudaStream_t s);
 int interact_grid_size(int lanes_per_particle, int n_init, int num_sms);
+
+// message returned by mfree_last_error() (mfree_host.cu)
+void set_last_error(const std::string &msg);
 
 // sustained FP32 FMA throughput of the current device in TFLOP/s (mfree_probe.cu)
 double fp32_peak_probe(int num_sms);
