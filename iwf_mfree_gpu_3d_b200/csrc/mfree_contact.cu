@@ -317,12 +317,23 @@ __global__ void __launch_bounds__(256) k_finalize(StepArgs a) {
     }
 }
 
-__global__ void k_force_final(StepArgs a, int num_blocks, float *out) {
-    const int c = threadIdx.x;
-    if (c >= 3 * a.p.num_tools || !a.clk->record) return;
-    float s = 0.f;
-    for (int b = 0; b < num_blocks; b++) s += a.s.force_part[size_t(b) * (3 * MAX_TOOLS) + c];
-    out[c] = s;
+// sum of the per-block partials: thread t adds blocks t, t+256, ... in order,
+// then a fixed tree over the 256 threads (deterministic for a given grid)
+__global__ void __launch_bounds__(256) k_force_final(StepArgs a, int num_blocks, float *out) {
+    if (!a.clk->record) return;
+    __shared__ float red[256];
+    for (int c = 0; c < 3 * a.p.num_tools; c++) {
+        float s = 0.f;
+        for (int b = threadIdx.x; b < num_blocks; b += 256) s += a.s.force_part[size_t(b) * (3 * MAX_TOOLS) + c];
+        red[threadIdx.x] = s;
+        __syncthreads();
+        for (int o = 128; o > 0; o >>= 1) {
+            if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[c] = red[0];
+        __syncthreads();
+    }
 }
 
 }  // namespace mfree

@@ -355,7 +355,7 @@ int enqueue_step(mfree_ctx *c, int record_mode, int record_every, bool timed = f
     run(8, [&] { le = launch_interact(a, lpp, interact_grid_size(lpp, c->n_init, c->num_sms), s); });
     if (le != cudaSuccess) return fail(MFREE_ERR_CUDA, std::string("pair kernel launch: ") + cudaGetErrorString(le));
     run(9, [&] { k_finalize<<<nb, 256, 0, s>>>(a); });
-    if (!c->tools.empty()) run(10, [&] { k_force_final<<<1, 32, 0, s>>>(a, nb, c->d_forces); });
+    if (!c->tools.empty()) run(10, [&] { k_force_final<<<1, 256, 0, s>>>(a, nb, c->d_forces); });
     CUDA_TRY(cudaGetLastError());
     return MFREE_OK;
 }

@@ -370,11 +370,19 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
     const float4 *__restrict__ rB = RF + REC_B * rstride;
     const float4 *__restrict__ rR = RF + REC_R * rstride;
     const float4 *__restrict__ rC = RF + REC_C * rstride;
+    // the target's cell; its own records come from the staged halo (its cell
+    // column is one of the halo's) or from global memory
+    const unsigned key = a.s.key_sorted[i];
+    const int nyz = ny * nz;
+    const int gi = int(key) / nyz, rem = int(key) - gi * nyz, gj = rem / nz, gk = rem - gj * nz;
     IData I;
     {
-        const Records &G_ = a.r;
-        const float4 Pi = G_.f[REC_P][i], Vi = G_.f[REC_V][i], Ai = G_.f[REC_A][i], Bi = G_.f[REC_B][i],
-                     Ri = G_.f[REC_R][i], Ci = G_.f[REC_C][i];
+        int si = i;
+        if (STAGED) {
+            const int lc = (gi - X0 + 2) * HY + (gj - Y0 + 2);
+            si = sm.hoff[lc] + (i - sm.hstart[lc]);
+        }
+        const float4 Pi = rP[si], Vi = rV[si], Ai = rA[si], Bi = rB[si], Ri = rR[si], Ci = rC[si];
         I.x = Pi.x; I.y = Pi.y; I.z = Pi.z; I.tool = Pi.w;
         I.vx = Vi.x; I.vy = Vi.y; I.vz = Vi.z; I.rho = Vi.w;
         I.s[0] = Ai.x; I.s[1] = Ai.y; I.s[2] = Ai.z; I.s[3] = Ai.w; I.s[4] = Bi.x; I.s[5] = Bi.y;
@@ -389,9 +397,6 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
     int *qq = sm.q[warp][g];
     // ---- the 25 stencil columns as ranges of the record arrays, with their prefix
     {
-        const unsigned key = a.s.key_sorted[i];
-        const int nyz = ny * nz;
-        const int gi = int(key) / nyz, rem = int(key) - gi * nyz, gj = rem / nz, gk = rem - gj * nz;
         const int klo = max(gk - 2, 0) - zl, khi = min(gk + 2, nz - 1) - zl + 1;
         constexpr int NSET = (25 + LPP - 1) / LPP;
         int carry = 0;
@@ -418,22 +423,45 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
         if (sl == 0) cp[25] = carry;
     }
     __syncwarp();
+    // ---- candidates: lane sl of the group scans the contiguous chunk
+    // [kb, ke) of the flattened stencil (columns in order); the column it is
+    // in and the record index advance in registers
     const int total = cp[25];
-    int maxtotal = total;
+    const int per = (total + LPP - 1) / LPP;
+    int maxper = per;
 #pragma unroll
-    for (int o = 16; o >= LPP; o >>= 1) maxtotal = max(maxtotal, __shfl_xor_sync(0xffffffffu, maxtotal, o));
+    for (int o = 16; o >= LPP; o >>= 1) maxper = max(maxper, __shfl_xor_sync(0xffffffffu, maxper, o));
+    const int kb = min(sl * per, total), ke = min(kb + per, total);
+    // visits the candidates of the chunk, one per step of the group, and
+    // calls fn(j, active) on every step (active false past the chunk's end)
+    auto scan = [&](auto &&fn) {
+        int col = 0;
+        while (col < 24 && cp[col + 1] <= kb) col++;
+        int cend = cp[col + 1];
+        int j = cb[col] + (kb - cp[col]);
+#pragma unroll 2
+        for (int it = 0; it < maxper; it++) {
+            const int k = kb + it;
+            const bool act = k < ke;
+            if (act) {
+                while (k >= cend) {  // next non-empty column (k < total keeps col <= 24)
+                    col++;
+                    cend = cp[col + 1];
+                    j = cb[col];
+                }
+            }
+            fn(j, act);
+            j++;
+        }
+    };
     // ---- pass A: support test, PSE, queue
     const float pse_k = -1.44269504088896341f * I.h1 * I.h1;  // exp(-r^2/h^2) = 2^(pse_k r^2)
     const float four_h2 = __fmul_rn(__fmul_rn(4.0f, I.h), I.h);
-    int col = 0, qn = 0, cnt = 0;
+    int qn = 0, cnt = 0;
     float pse = 0.f;
-    for (int k0 = 0; k0 < maxtotal; k0 += LPP) {
-        const int k = k0 + sl;
+    scan([&](int j, bool act) {
         bool ins = false;
-        int j = 0;
-        if (k < total) {
-            while (cp[col + 1] <= k) col++;
-            j = cb[col] + (k - cp[col]);
+        if (act) {
             const float4 Pj = rP[j];
             const float dx = I.x - Pj.x, dy = I.y - Pj.y, dz = I.z - Pj.z;
             const float r2 = dist2_rn(dx, dy, dz);
@@ -450,23 +478,19 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
             if (pos < QCAP_T) qq[pos] = j;
         }
         qn += __popc(m);
-    }
+    });
     __syncwarp();
     const int qv = min(qn, QCAP_T);
     int maxq = qv;
 #pragma unroll
     for (int o = 16; o >= LPP; o >>= 1) maxq = max(maxq, __shfl_xor_sync(0xffffffffu, maxq, o));
     const bool overflow = __any_sync(0xffffffffu, qn > QCAP_T);
-    // in-support neighbours beyond the queue: found again by rescanning
+    // in-support neighbours beyond the queue: found again by the same scan
     auto for_overflow = [&](auto &&fn) {
-        int col2 = 0, ord = 0;
-        for (int k0 = 0; k0 < maxtotal; k0 += LPP) {
-            const int k = k0 + sl;
+        int ord = 0;
+        scan([&](int j, bool act) {
             bool ins = false;
-            int j = 0;
-            if (k < total && qn > QCAP_T) {
-                while (cp[col2 + 1] <= k) col2++;
-                j = cb[col2] + (k - cp[col2]);
+            if (act && qn > QCAP_T) {
                 const float4 Pj = rP[j];
                 ins = in_support(dist2_rn(I.x - Pj.x, I.y - Pj.y, I.z - Pj.z), I.h);
             }
@@ -474,7 +498,7 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
             const int pos = ord + __popc(m & lt_mask);
             if (ins && pos >= QCAP_T) fn(j);
             ord += __popc(m);
-        }
+        });
     };
     // ---- CSPM matrix over the in-support neighbours (interactions_gpu.cu:227-295)
     float invB[9] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};
@@ -698,12 +722,15 @@ __global__ void __launch_bounds__(TILE_THREADS, 1) k_interact(StepArgs a, int nt
                     done += TILE_WARPS * G;
                 }
             }
+            // the rounds were the last generic reads of the staged halo: order
+            // them before the next tile's bulk writes (the barriers that follow
+            // carry the order to the threads that issue the copies)
+            fence_proxy_async();
             __syncthreads();
             // ---- per-particle rest of the step, one thread per target
             for (int tt = threadIdx.x; tt < tn; tt += TILE_THREADS) epilogue<PREC, COND>(a, sm.tgt[tt], sm.res[tt]);
             __syncthreads();
         }
-        fence_proxy_async();  // generic reads of the staged halo precede the next tile's bulk writes
     }
 }
 
