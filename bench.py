@@ -309,7 +309,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     roofline = {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
                 "frac": achieved / peak_fp32,
                 "traffic": traffic,
-                "kernel": "k_interact (pair loop + fused per-particle rest of the step)",
+                "kernel": "kb_interact (pair loop + fused per-particle rest of the step)",
                 "peak_source": "measured: FP32 FMA-throughput probe on this GPU (mfree_probe_fp32_peak); "
                                "MEASURED_PEAKS.json holds HBM and bf16 tensor peaks only",
                 "algorithmic_flops_per_launch": flops_launch,

@@ -43,6 +43,8 @@ extern "C" {
 #define MFREE_ERR_EMPTY      -6  /* every particle left the box: the
                                     reference prints and exit(0)s
                                     (grid_gpu_base.cu:159-163)            */
+#define MFREE_ERR_BUDGET     -7  /* admitting the scene would exceed the
+                                    batch's device-memory budget          */
 
 /* ---- constant records (constants_structs.h:25-92) ----------------------- */
 typedef struct { float E, nu, rho0, K, G, mass; } mfree_phys;          /* phys_constants */
@@ -68,6 +70,8 @@ typedef struct {
     int friction_tool_vel;  /* 1: subtract the tool velocity in the friction slip
                                velocity.  The reference never uploads its tool_vel
                                constant (tool_3d_gpu.cu:26,528), so 0 matches it.    */
+    int tile_depth;         /* pair-loop tiling: cells per tile along z, 1..8; 0 picks
+                               the tuned default (6).  Results do not depend on it.   */
 } mfree_options;
 
 /* ---- fields for mfree_get_field / mfree_set_field ------------------------
@@ -268,6 +272,63 @@ int mfree_set_device(int device);
 #define MFREE_STATIC_MAX_CELLS     524288
 int mfree_cell_list_static(const float *pos4, int n, const float bbmin[3], float dx, int nx, int ny, int nz,
                            int *perm, int *cell_first, void *stream);
+
+/* ---- batches: many scenes stepped together ------------------------------
+ * The reference runs one scene per process (main(), mfree_gpu_3d.cpp:75-218);
+ * these calls have no counterpart there.  A batch holds independent scenes
+ * of any sizes (each an mfree_ctx, configured as for mfree_step) and steps
+ * all of them with one launch per kernel: every scene keeps its own state and
+ * cell list, and a scene's results are the same alone and in a batch when the
+ * pair-loop tiling is the same.  Scenes are admitted and retired between
+ * steps (continuous batching): admission is bounded by a device-memory
+ * budget, and a scene may be admitted with a step count after which it stops.
+ * All scenes of a batch share the pair-kernel variant (cspm, conduction,
+ * precision options) and the tiling (lanes per particle, tile depth). */
+typedef struct mfree_batch mfree_batch;
+
+/* hbm_budget: device bytes the admitted scenes may hold (0: no limit).
+ * stream: cudaStream_t, or NULL for a stream of the batch's own. */
+int mfree_batch_create(size_t hbm_budget, void *stream, mfree_batch **out);
+/* destroys the batch and every context it still holds */
+int mfree_batch_destroy(mfree_batch *b);
+/* Admits a configured context; on success the batch owns it (its work moves to
+ * the batch's stream and mfree_step/mfree_advance on it are refused until it
+ * is retired).  steps > 0: the scene stops after that many batch steps
+ * (status done); steps <= 0: it runs until retired.  MFREE_ERR_BUDGET: its
+ * device memory does not fit the budget (the caller keeps the context).
+ * MFREE_ERR_ARG: its pair-kernel variant differs from the batch's. */
+int mfree_batch_admit(mfree_batch *b, mfree_ctx *ctx, long long steps, int *slot);
+/* Advances every running scene by up to nsteps steps (a scene stops at its
+ * step count; the others go on).  record_every > 0: tool forces are recorded
+ * on steps whose index is a multiple of it.  use_graph: each step replays one
+ * captured CUDA graph covering all scenes (re-captured when scenes join or
+ * leave). */
+int mfree_batch_step(mfree_batch *b, int nsteps, int record_every, int use_graph);
+/* slot state: *done steps run, *target requested (<= 0: unbounded),
+ * *status 0 running, 1 done, 2 free slot, < 0 the scene's error status */
+int mfree_batch_query(mfree_batch *b, int slot, long long *done, long long *target, int *status);
+/* the slot's context, for the field and force calls (the batch still owns it) */
+int mfree_batch_context(mfree_batch *b, int slot, mfree_ctx **ctx);
+/* Removes a scene.  ctx != NULL: ownership returns to the caller (on its
+ * original stream); ctx == NULL: the context is destroyed. */
+int mfree_batch_retire(mfree_batch *b, int slot, mfree_ctx **ctx);
+/* scenes held, running scenes, device bytes held by them and the budget */
+int mfree_batch_info(mfree_batch *b, int *scenes, int *running, size_t *bytes, size_t *budget);
+/* Pair-loop tiling of the batch: lanes per particle (8, 16, 32) and tile depth
+ * (1..8 cells); 0 keeps the current value. */
+int mfree_batch_set_tiling(mfree_batch *b, int lanes_per_particle, int tile_depth);
+int mfree_batch_get_tiling(mfree_batch *b, int *lanes_per_particle, int *tile_depth);
+/* Autotuner: times every tiling (lanes per particle x tile depth 4..8) for
+ * trial_steps steps on copies of the batch's running scenes (their own state
+ * is untouched) and keeps the fastest.  The cell size stays the reference's
+ * (the smoothing length), which the bit-exact cell ids and order require.
+ * *ms_best: time per step of the chosen tiling (may be NULL). */
+int mfree_batch_autotune(mfree_batch *b, int trial_steps, int *lanes_per_particle, int *tile_depth, double *ms_best);
+/* device bytes a context holds (state, scratch and tools) */
+int mfree_device_bytes(const mfree_ctx *ctx, size_t *bytes);
+/* device bytes mfree_create + mfree_set_grid will take for n particles and
+ * num_cell grid cells, before tools: to check a budget before creating */
+size_t mfree_scene_bytes(int n, long long num_cell);
 
 /* ---- scene files (the reference's setup readers) ------------------------- */
 /* json_read_triangles (json_reader.cpp:108-117): MeshLab JSON */

@@ -39,8 +39,11 @@ EXPORTS = [
     "mfree_get_field_f64", "mfree_get_cells", "mfree_get_grid", "mfree_get_counters", "mfree_read_mesh_json",
     "mfree_read_mesh_ldynak", "mfree_free", "mfree_set_kernel_timing", "mfree_get_kernel_times",
     "mfree_probe_fp32_peak", "mfree_timer_start", "mfree_timer_stop", "mfree_set_device",
-    "mfree_cell_list_static",
+    "mfree_cell_list_static", "mfree_batch_create", "mfree_batch_destroy", "mfree_batch_admit", "mfree_batch_step",
+    "mfree_batch_query", "mfree_batch_context", "mfree_batch_retire", "mfree_batch_info", "mfree_batch_set_tiling",
+    "mfree_batch_get_tiling", "mfree_batch_autotune", "mfree_device_bytes", "mfree_scene_bytes",
 ]
+ERR_BUDGET = -7
 KERNELS = ["clock", "hash", "scan_reduce", "scan_top", "scan_down", "scatter", "cell_fixup", "gather_predict",
            "interact", "finalize", "force_final"]
 
@@ -69,7 +72,8 @@ class Joco(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("cspm", "conduction", "precision", "max_secant_iter",
-                                       "lanes_per_particle", "diagnostics", "friction_tool_vel")]
+                                       "lanes_per_particle", "diagnostics", "friction_tool_vel",
+                                       "tile_depth")]
 
 
 class Counters(C.Structure):
@@ -133,6 +137,21 @@ def lib(path: str = LIB_PATH):
     L.mfree_timer_stop.argtypes = [P, C.POINTER(C.c_double)]
     L.mfree_set_device.argtypes = [I]
     L.mfree_cell_list_static.argtypes = [P, I, fp, F, I, I, I, P, P, P]
+    S, LL = C.c_size_t, C.c_longlong
+    L.mfree_batch_create.argtypes = [S, P, C.POINTER(P)]
+    L.mfree_batch_destroy.argtypes = [P]
+    L.mfree_batch_admit.argtypes = [P, P, LL, ip]
+    L.mfree_batch_step.argtypes = [P, I, I, I]
+    L.mfree_batch_query.argtypes = [P, I, C.POINTER(LL), C.POINTER(LL), ip]
+    L.mfree_batch_context.argtypes = [P, I, C.POINTER(P)]
+    L.mfree_batch_retire.argtypes = [P, I, C.POINTER(P)]
+    L.mfree_batch_info.argtypes = [P, ip, ip, C.POINTER(S), C.POINTER(S)]
+    L.mfree_batch_set_tiling.argtypes = [P, I, I]
+    L.mfree_batch_get_tiling.argtypes = [P, ip, ip]
+    L.mfree_batch_autotune.argtypes = [P, I, ip, ip, C.POINTER(C.c_double)]
+    L.mfree_device_bytes.argtypes = [P, C.POINTER(S)]
+    L.mfree_scene_bytes.argtypes = [I, LL]
+    L.mfree_scene_bytes.restype = S
     _lib = L
     return L
 
@@ -229,7 +248,7 @@ class Simulation:
 
     def set_options(self, **kw):
         o = Options(cspm=0, conduction=COND_BROOKSHAW, precision=0, max_secant_iter=100, lanes_per_particle=0,
-                    diagnostics=0, friction_tool_vel=0)
+                    diagnostics=0, friction_tool_vel=0, tile_depth=0)
         for k, v in kw.items():
             setattr(o, k, int(v))
         self._opt = o
@@ -382,7 +401,15 @@ class Simulation:
         _check(self.L.mfree_get_cells(self.h, cs.ctypes.data_as(ip), ce.ctypes.data_as(ip)))
         return cs, ce
 
+    def device_bytes(self) -> int:
+        """Device memory the context holds (state, scratch, tools)."""
+        b = C.c_size_t()
+        _check(self.L.mfree_device_bytes(self.h, C.byref(b)))
+        return b.value
+
     def close(self):
+        if getattr(self, "_batch", None) is not None:
+            return  # a batch owns the context; Batch.retire / Batch.close release it
         if getattr(self, "h", None) is not None and self.h.value:
             self.L.mfree_destroy(self.h)
             self.h = C.c_void_p()
@@ -416,3 +443,91 @@ class Simulation:
         dt = np.float32(scene.dt)
         s.set_time(float(dt), float(np.float32(0) + dt))
         return s
+
+
+def scene_bytes(n: int, num_cell: int) -> int:
+    """Device bytes mfree_create + mfree_set_grid take for n particles and num_cell cells (tools excluded)."""
+    return int(lib().mfree_scene_bytes(int(n), int(num_cell)))
+
+
+class Batch:
+    """Independent scenes stepped together, one launch per kernel (mfree_batch_*).
+
+    ``admit`` hands a configured ``Simulation`` to the batch (field reads keep
+    working on it); ``step`` advances every running scene; a scene admitted
+    with ``steps`` stops after that many steps; ``retire`` removes it.
+    """
+    RUNNING, DONE, FREE = 0, 1, 2
+
+    def __init__(self, hbm_budget: int = 0, stream: Optional[int] = None):
+        self.L = lib()
+        h = C.c_void_p()
+        _check(self.L.mfree_batch_create(int(hbm_budget), C.c_void_p(stream) if stream else None, C.byref(h)))
+        self.h = h
+        self.sims = {}
+
+    def admit(self, sim: Simulation, steps: int = 0) -> Optional[int]:
+        """Slot of the admitted scene, or None when it does not fit the memory budget."""
+        k = C.c_int()
+        st = self.L.mfree_batch_admit(self.h, sim.h, int(steps), C.byref(k))
+        if st == ERR_BUDGET:
+            return None
+        _check(st)
+        sim._batch = self
+        self.sims[k.value] = sim
+        return k.value
+
+    def step(self, nsteps: int = 1, record_every: int = 0, use_graph: bool = True):
+        _check(self.L.mfree_batch_step(self.h, int(nsteps), int(record_every), int(use_graph)))
+
+    def query(self, slot: int):
+        """(steps done, steps requested, status): status 0 running, 1 done, 2 free, < 0 error."""
+        d, t, s = C.c_longlong(), C.c_longlong(), C.c_int()
+        _check(self.L.mfree_batch_query(self.h, int(slot), C.byref(d), C.byref(t), C.byref(s)))
+        return d.value, t.value, s.value
+
+    def retire(self, slot: int, keep: bool = False) -> Optional[Simulation]:
+        """Remove a scene; keep=True returns its Simulation (owned by the caller again)."""
+        sim = self.sims.pop(int(slot))
+        out = C.c_void_p()
+        _check(self.L.mfree_batch_retire(self.h, int(slot), C.byref(out) if keep else None))
+        sim._batch = None
+        if keep:
+            return sim
+        sim.h = C.c_void_p()
+        return None
+
+    def info(self) -> dict:
+        n, r = C.c_int(), C.c_int()
+        b, bud = C.c_size_t(), C.c_size_t()
+        _check(self.L.mfree_batch_info(self.h, C.byref(n), C.byref(r), C.byref(b), C.byref(bud)))
+        return dict(scenes=n.value, running=r.value, bytes=b.value, budget=bud.value)
+
+    def set_tiling(self, lanes_per_particle: int = 0, tile_depth: int = 0):
+        _check(self.L.mfree_batch_set_tiling(self.h, int(lanes_per_particle), int(tile_depth)))
+
+    def tiling(self):
+        a, b = C.c_int(), C.c_int()
+        _check(self.L.mfree_batch_get_tiling(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def autotune(self, trial_steps: int = 3):
+        """Time every tiling on copies of the running scenes; keep the fastest: (lanes, depth, ms/step)."""
+        a, b, ms = C.c_int(), C.c_int(), C.c_double()
+        _check(self.L.mfree_batch_autotune(self.h, int(trial_steps), C.byref(a), C.byref(b), C.byref(ms)))
+        return a.value, b.value, ms.value
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.L.mfree_batch_destroy(self.h)
+            for sim in self.sims.values():
+                sim._batch = None
+                sim.h = C.c_void_p()
+            self.sims = {}
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

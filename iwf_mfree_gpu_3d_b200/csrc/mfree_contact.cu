@@ -178,9 +178,9 @@ __device__ void closest_by_shells(const ToolDev &T, const ToolClock &B, float t,
 
 // one thread per particle; particles of the blanked tail only translate if
 // they are tool particles
-__global__ void __launch_bounds__(256) k_finalize(StepArgs a) {
+__device__ __forceinline__ void finalize_body(const StepArgs &a, int bid) {
     const Params &P = a.p;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = bid * 256 + threadIdx.x;
     const int N = a.clk->n_active;
     const bool rec = a.clk->record != 0;
     const State &S = a.b;
@@ -312,14 +312,14 @@ __global__ void __launch_bounds__(256) k_finalize(StepArgs a) {
     __syncthreads();
     if (threadIdx.x < 3 * P.num_tools) {
         float s = 0.f;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w][threadIdx.x];
-        a.s.force_part[size_t(blockIdx.x) * (3 * MAX_TOOLS) + threadIdx.x] = s;
+        for (int w = 0; w < 8; w++) s += red[w][threadIdx.x];
+        a.s.force_part[size_t(bid) * (3 * MAX_TOOLS) + threadIdx.x] = s;
     }
 }
 
 // sum of the per-block partials: thread t adds blocks t, t+256, ... in order,
 // then a fixed tree over the 256 threads (deterministic for a given grid)
-__global__ void __launch_bounds__(256) k_force_final(StepArgs a, int num_blocks, float *out) {
+__device__ __forceinline__ void force_final_body(const StepArgs &a, int num_blocks, float *out) {
     if (!a.clk->record) return;
     __shared__ float red[256];
     for (int c = 0; c < 3 * a.p.num_tools; c++) {
@@ -334,6 +334,21 @@ __global__ void __launch_bounds__(256) k_force_final(StepArgs a, int num_blocks,
         if (threadIdx.x == 0) out[c] = red[0];
         __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(256) kb_finalize(BatchTable T) {
+    __shared__ StepArgs sa;
+    const int s = find_scene(T.pblk, T.nscenes, blockIdx.x);
+    load_scene_args(sa, T, s);
+    __syncthreads();
+    finalize_body(sa, int(blockIdx.x) - T.pblk[s]);
+}
+// one block per scene
+__global__ void __launch_bounds__(256) kb_force_final(BatchTable T) {
+    __shared__ StepArgs sa;
+    load_scene_args(sa, T, blockIdx.x);
+    __syncthreads();
+    if (sa.p.num_tools > 0) force_final_body(sa, (sa.p.n_init + 255) / 256, sa.s.forces);
 }
 
 }  // namespace mfree

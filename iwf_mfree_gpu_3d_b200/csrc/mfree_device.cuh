@@ -34,6 +34,7 @@
 namespace mfree {
 
 constexpr int MAX_TOOLS = 8;
+constexpr int TILE_Z_MAX = 8;  // largest pair-kernel tile depth (cells along z)
 
 // time-varying scalars kept on the device so a step can be replayed from a
 // CUDA graph: the clock kernel advances them at the start of every step
@@ -45,8 +46,8 @@ struct DevClock {
     int pending;      // 1 once a step has run: the next clock tick adds dt first
     int n_active;     // N (particles not blanked), written by the scan
     int record;       // record tool forces this step
-    int tile_next;    // work queue of the pair kernel (reset by the clock kernel)
     int tile_error;   // staging waits that ran out (the tile fell back to global reads)
+    int parity;       // which of the two state copies holds this step's input (flips every step)
     long long step_index;
     float blank_min[3], blank_max[3];
     float grid_min[3];
@@ -98,6 +99,7 @@ struct Params {
     int num_tools;
     float tool0_vel[3];  // global_tool[0]->get_vel(): friction heat and tool particles
     int record_every;
+    int tile_z;  // cells per pair-kernel tile along z (1..TILE_Z_MAX)
 };
 
 struct State {
@@ -125,9 +127,10 @@ struct Scratch {
     float4 *pos_half;      // half-step positions (diagnostics)
     float4 *nrm;           // contact normal (diagnostics)
     float *force_part;     // per-block partial tool forces (3 per tool per block)
+    float *forces;         // per-tool force of the last recorded step (3 per tool)
 };
 
-struct StepArgs {
+struct alignas(16) StepArgs {
     Params p;
     State a, b;   // a = state before the sort, b = sorted state
     Records r;

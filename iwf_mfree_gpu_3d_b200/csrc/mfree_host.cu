@@ -17,100 +17,24 @@
 #include <string>
 #include <vector>
 
-#include "mfree.h"
-#include "mfree_kernels.cuh"
-#include "mfree_tool.h"
+#include "mfree_ctx.h"
 
 using namespace mfree;
+using namespace mfree::host;
 
 namespace {
-
 thread_local std::string g_err;
+}  // namespace
 
-int fail(int code, const std::string &msg) {
+int mfree::host::fail(int code, const std::string &msg) {
     g_err = msg;
     return code;
 }
 
-}  // namespace
-
 void mfree::set_last_error(const std::string &msg) { g_err = msg; }
 
-namespace {
-
-#define CUDA_TRY(x)                                                                        \
-    do {                                                                                   \
-        cudaError_t e_ = (x);                                                              \
-        if (e_ != cudaSuccess)                                                             \
-            return fail(e_ == cudaErrorMemoryAllocation ? MFREE_ERR_OOM : MFREE_ERR_CUDA,  \
-                        std::string(#x) + ": " + cudaGetErrorString(e_));                 \
-    } while (0)
-
-struct DevTool {
-    HostTool host;
-    int algorithm = MFREE_CONTACT_HASHED;
-    float vel[3] = {0, 0, 0};
-    float alpha = 0.1f, mu = 0.f;
-    float birth = -3.402823466e+38f, death = 3.402823466e+38f;
-    float4 *d_tri = nullptr;  // 10 arrays of float4, back to back
-    int *d_cells = nullptr;
-    int ntri_dev = 0;
-};
-
-}  // namespace
-
-struct mfree_ctx {
-    int n_init = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    int device = 0, num_sms = 148;
-    // host-side configuration
-    mfree_phys phys{};
-    mfree_corr corr{};
-    mfree_joco joco{};
-    mfree_trml twp{}, ttool{};
-    mfree_options opt{};
-    bool plastic = false;
-    bool grid_set = false;
-    float g_bbmin[3], g_bbmax[3], g_dx = 0.f, g_vel[3] = {0, 0, 0};
-    long nx = 0, ny = 0, nz = 0, num_cell = 0;
-    bool blank_set = false;
-    float b_min[3], b_max[3], b_vel[3] = {0, 0, 0}, b_vmax = 0.f;
-    float dt = 0.f, t = 0.f;
-    bool time_set = false;
-    std::vector<std::unique_ptr<DevTool>> tools;
-    // device memory
-    State st[2]{};
-    int cur = 0;
-    Records rec{};
-    Scratch scr{};
-    DevClock *d_clk = nullptr;
-    float *d_forces = nullptr;
-    size_t scratch_cells = 0;  // num_cell the scratch was sized for
-    std::vector<void *> allocs, scratch_allocs;
-    bool clock_dirty = true;  // host-side scalars changed: rewrite the device clock
-    bool pending = false;     // a step has run since the clock was written
-    long long steps = 0;
-    // per-kernel timing (eager steps)
-    bool timing = false;
-    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> tev;
-    std::vector<cudaEvent_t> event_pool;
-    double kernel_ms[MFREE_NUM_KERNELS] = {0};
-    int kernel_n[MFREE_NUM_KERNELS] = {0};
-    cudaEvent_t timer[2] = {nullptr, nullptr};
-    // active count of the last step, copied back asynchronously: a step that
-    // left no particle makes the next call return MFREE_ERR_EMPTY (the
-    // reference exits there, grid_gpu_base.cu:159-163)
-    int *h_nact = nullptr;
-    cudaEvent_t nact_ev = nullptr;
-    bool nact_pending = false;
-    // graphs, one per state parity
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    int graph_record_every = -1;
-    bool graph_valid = false;
-};
-
-namespace {
+namespace mfree {
+namespace host {
 
 template <class T> int dalloc(mfree_ctx *c, T **p, size_t n, std::vector<void *> &list) {
     void *q = nullptr;
@@ -118,9 +42,11 @@ template <class T> int dalloc(mfree_ctx *c, T **p, size_t n, std::vector<void *>
     if (e != cudaSuccess) return fail(MFREE_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     list.push_back(q);
     *p = (T *)q;
-    (void)c;
+    (&list == &c->scratch_allocs ? c->scratch_bytes : c->bytes) += std::max<size_t>(n, 1) * sizeof(T);
     return MFREE_OK;
 }
+
+size_t device_bytes(const mfree_ctx *c) { return c->bytes + c->scratch_bytes; }
 
 void free_list(std::vector<void *> &l) {
     for (void *p : l) cudaFree(p);
@@ -128,15 +54,14 @@ void free_list(std::vector<void *> &l) {
 }
 
 void invalidate_graphs(mfree_ctx *c) {
-    for (auto &g : c->graph)
-        if (g) {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-        }
-    c->graph_valid = false;
+    c->version++;
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+    c->graph_record_every = -1;
 }
 
 int default_lpp() { return 8; }
+int default_tile_depth() { return 6; }
 
 Params make_params(const mfree_ctx *c) {
     Params P{};
@@ -199,6 +124,7 @@ Params make_params(const mfree_ctx *c) {
     P.num_tools = int(c->tools.size());
     for (int d = 0; d < 3; d++) P.tool0_vel[d] = c->tools.empty() ? 0.f : c->tools[0]->vel[d];
     P.record_every = 0;
+    P.tile_z = c->opt.tile_depth > 0 ? c->opt.tile_depth : default_tile_depth();
     return P;
 }
 
@@ -247,6 +173,7 @@ StepArgs make_args(mfree_ctx *c) {
 int ensure_scratch(mfree_ctx *c) {
     if (c->scratch_cells == size_t(c->num_cell) && !c->scratch_allocs.empty()) return MFREE_OK;
     free_list(c->scratch_allocs);
+    c->scratch_bytes = 0;
     auto &L = c->scratch_allocs;
     int st;
     if ((st = dalloc(c, &c->scr.count, c->num_cell + 1, L))) return st;
@@ -265,6 +192,7 @@ int write_clock(mfree_ctx *c) {
     h.n_active = c->n_init;
     h.record = 0;
     h.step_index = c->steps;
+    h.parity = c->cur;
     for (int d = 0; d < 3; d++) {
         h.blank_min[d] = c->b_min[d];
         h.blank_max[d] = c->b_max[d];
@@ -300,11 +228,13 @@ int ready(mfree_ctx *c) {
     if (lpp != 0 && lpp != 8 && lpp != 16 && lpp != 32)
         return fail(MFREE_ERR_ARG, "lanes_per_particle must be 0, 8, 16 or 32");
     if (c->opt.conduction < 0 || c->opt.conduction > 2) return fail(MFREE_ERR_ARG, "bad conduction mode");
+    if (c->opt.tile_depth < 0 || c->opt.tile_depth > TILE_Z_MAX) return fail(MFREE_ERR_ARG, "tile_depth must be 0..8");
     int st = ensure_scratch(c);
     if (st) return st;
     {
-        StepArgs a = make_args(c);
-        cudaError_t e = launch_interact(a, lpp ? lpp : default_lpp(), 0, c->stream);
+        const StepArgs a = make_args(c);
+        cudaError_t e = launch_interact_batch(BatchTable{}, lpp ? lpp : default_lpp(), a.p.cspm != 0, a.p.conduction,
+                                              a.p.precision != 0, 0, c->stream);
         if (e != cudaSuccess) return fail(MFREE_ERR_CUDA, std::string("pair kernel setup: ") + cudaGetErrorString(e));
     }
     if (c->clock_dirty) return write_clock(c);
@@ -322,10 +252,53 @@ cudaEvent_t pooled_event(mfree_ctx *c) {
     return e;
 }
 
-// the kernels of one step; record_mode as k_clock
+// The context's one-scene table: its step arguments for both state parities
+// (the clock kernel flips the parity on the device) and the block counts of
+// each kernel family.  A single scene runs the batched kernels over this
+// table, so its arithmetic is the same compiled code alone and in a batch.
+// Uploaded again only when the arguments may have changed (setters bump the
+// context's version); never inside a stream capture.
+int ensure_table(mfree_ctx *c, int record_every) {
+    if (c->d_table && c->table_version == c->version && c->table_record_every == record_every) return MFREE_OK;
+    if (!c->d_table) {
+        int st = dalloc(c, &c->d_table, single_table_bytes(), c->allocs);
+        if (st) return st;
+    }
+    StepArgs args[2];
+    const int keep = c->cur;
+    for (int p = 0; p < 2; p++) {
+        c->cur = p;
+        args[p] = make_args(c);
+        args[p].p.record_every = record_every;
+    }
+    c->cur = keep;
+    const Params &P = args[0].p;
+    const int ntiles = ((P.gnx + 3) / 4) * ((P.gny + 3) / 4) * ((P.gnz + P.tile_z - 1) / P.tile_z);
+    const int pre[9] = {0, hash_blocks(c), 0, scan_tiles(c), 0, int((c->num_cell + 255) / 256), 0, ntiles, 0};
+    StepArgs *da = (StepArgs *)c->d_table;
+    int *di = (int *)(da + 2);
+    // pageable sources: the call returns once the bytes are staged
+    CUDA_TRY(cudaMemcpyAsync(da, args, sizeof(args), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(di, pre, sizeof(pre), cudaMemcpyHostToDevice, c->stream));
+    c->T.args = da;
+    c->T.pblk = di;
+    c->T.stile = di + 2;
+    c->T.cblk = di + 4;
+    c->T.itile = di + 6;
+    c->T.tile_next = di + 8;
+    c->T.nscenes = 1;
+    c->table_version = c->version;
+    c->table_record_every = record_every;
+    return MFREE_OK;
+}
+
+// the kernels of one step; record_mode as kb_clock (2: every record_every
+// steps of the scene's step index)
 int enqueue_step(mfree_ctx *c, int record_mode, int record_every, bool timed = false) {
-    StepArgs a = make_args(c);
-    a.p.record_every = record_every;
+    int st = ensure_table(c, record_every);
+    if (st) return st;
+    const BatchTable &T = c->T;
+    const Params &P = make_args(c).p;
     cudaStream_t s = c->stream;
     const int hb = hash_blocks(c), tiles = scan_tiles(c);
     const int nb = (c->n_init + 255) / 256;
@@ -344,18 +317,19 @@ int enqueue_step(mfree_ctx *c, int record_mode, int record_every, bool timed = f
             c->tev.push_back({id, {e0, e1}});
         }
     };
-    run(0, [&] { k_clock<<<1, 32, 0, s>>>(a, record_mode); });
-    run(1, [&] { k_hash<<<hb, HASH_BLOCK, 0, s>>>(a); });
-    run(2, [&] { k_scan_reduce<<<tiles, SCAN_THREADS, 0, s>>>(a); });
-    run(3, [&] { k_scan_top<<<1, 1024, 0, s>>>(a, tiles, hb); });
-    run(4, [&] { k_scan_down<<<tiles, SCAN_THREADS, 0, s>>>(a); });
-    run(5, [&] { k_scatter<<<hb, HASH_BLOCK, 0, s>>>(a); });
-    run(6, [&] { k_cell_fixup<<<int((c->num_cell + 255) / 256), 256, 0, s>>>(a); });
-    run(7, [&] { launch_gather_predict(a, nb, s); });
-    run(8, [&] { le = launch_interact(a, lpp, interact_grid_size(lpp, c->n_init, c->num_sms), s); });
-    if (le != cudaSuccess) return fail(MFREE_ERR_CUDA, std::string("pair kernel launch: ") + cudaGetErrorString(le));
-    run(9, [&] { k_finalize<<<nb, 256, 0, s>>>(a); });
-    if (!c->tools.empty()) run(10, [&] { k_force_final<<<1, 256, 0, s>>>(a, nb, c->d_forces); });
+    run(0, [&] { kb_clock<<<1, 32, 0, s>>>(T, record_mode); });
+    run(1, [&] { kb_hash<<<hb, HASH_BLOCK, 0, s>>>(T); });
+    run(2, [&] { kb_scan_reduce<<<tiles, SCAN_THREADS, 0, s>>>(T); });
+    run(3, [&] { kb_scan_top<<<1, 1024, 0, s>>>(T); });
+    run(4, [&] { kb_scan_down<<<tiles, SCAN_THREADS, 0, s>>>(T); });
+    run(5, [&] { kb_scatter<<<hb, HASH_BLOCK, 0, s>>>(T); });
+    run(6, [&] { kb_cell_fixup<<<int((c->num_cell + 255) / 256), 256, 0, s>>>(T); });
+    run(7, [&] { le = launch_gather_predict_batch(T, P.precision != 0, nb, s); });
+    if (le == cudaSuccess)
+        run(8, [&] { le = launch_interact_batch(T, lpp, P.cspm != 0, P.conduction, P.precision != 0, c->num_sms, s); });
+    if (le != cudaSuccess) return fail(MFREE_ERR_CUDA, std::string("step launch: ") + cudaGetErrorString(le));
+    run(9, [&] { kb_finalize<<<nb, 256, 0, s>>>(T); });
+    if (!c->tools.empty()) run(10, [&] { kb_force_final<<<1, 256, 0, s>>>(T); });
     CUDA_TRY(cudaGetLastError());
     return MFREE_OK;
 }
@@ -378,7 +352,155 @@ int copy_field_raw(mfree_ctx *c, const float4 *src, std::vector<float4> &dst) {
     return MFREE_OK;
 }
 
-}  // namespace
+int check_empty(mfree_ctx *c, bool wait) {
+    if (!c->nact_pending) return MFREE_OK;
+    if (!wait && cudaEventQuery(c->nact_ev) != cudaSuccess) return MFREE_OK;
+    CUDA_TRY(cudaEventSynchronize(c->nact_ev));
+    c->nact_pending = false;
+    if (*c->h_nact == 0) return fail(MFREE_ERR_EMPTY, "all particles are blanked (outside the blanking box)");
+    return MFREE_OK;
+}
+
+int note_active_count(mfree_ctx *c) {
+    if (!c->h_nact) {
+        CUDA_TRY(cudaMallocHost(&c->h_nact, sizeof(int)));
+        CUDA_TRY(cudaEventCreateWithFlags(&c->nact_ev, cudaEventDisableTiming));
+    }
+    CUDA_TRY(cudaMemcpyAsync(c->h_nact, &c->d_clk->n_active, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaEventRecord(c->nact_ev, c->stream));
+    c->nact_pending = true;
+    return MFREE_OK;
+}
+
+// device memory of a context: both state copies, the neighbour records, the
+// per-particle scratch, the clock and the force outputs (the grid-sized
+// scratch follows in ensure_scratch)
+int alloc_ctx(int n, cudaStream_t stream, std::unique_ptr<mfree_ctx> &out) {
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    auto c = std::make_unique<mfree_ctx>();
+    c->n_init = n;
+    c->stream = stream;
+    if (!c->stream) {  // own stream: graph capture is not allowed on the legacy default stream
+        CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    c->device = dev;
+    CUDA_TRY(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev));
+    c->opt.max_secant_iter = 100;
+    auto &L = c->allocs;
+    auto bail = [&](int st) {
+        free_list(c->allocs);
+        if (c->own_stream) cudaStreamDestroy(c->stream);
+        return st;
+    };
+    int st;
+    for (int b = 0; b < 2; b++) {
+        State &S = c->st[b];
+        float4 **f[] = {&S.pos4, &S.vel4, &S.sa4, &S.sb4, &S.da4, &S.dv4, &S.dsa4, &S.dsb4,
+                        &S.fc4, &S.ft4, &S.bc4, &S.lo4, &S.lo4b};
+        for (auto p : f)
+            if ((st = dalloc(c.get(), p, n, L))) return bail(st);
+    }
+    {
+        float4 *base = nullptr;
+        if ((st = dalloc(c.get(), &base, size_t(REC_N) * n, L))) return bail(st);
+        for (int k = 0; k < REC_N; k++) c->rec.f[k] = base + size_t(k) * n;
+    }
+    if ((st = dalloc(c.get(), &c->scr.key, n, L))) return bail(st);
+    if ((st = dalloc(c.get(), &c->scr.key_sorted, n, L))) return bail(st);
+    if ((st = dalloc(c.get(), &c->scr.perm, n, L))) return bail(st);
+    if ((st = dalloc(c.get(), &c->scr.blank_block, (n + HASH_BLOCK - 1) / HASH_BLOCK + 1, L))) return bail(st);
+    if ((st = dalloc(c.get(), &c->scr.nnb, n, L))) return bail(st);
+    if ((st = dalloc(c.get(), &c->scr.pos_half, n, L))) return bail(st);
+    if ((st = dalloc(c.get(), &c->scr.nrm, n, L))) return bail(st);
+    if ((st = dalloc(c.get(), &c->scr.force_part, size_t((n + 255) / 256) * 3 * MAX_TOOLS, L))) return bail(st);
+    if ((st = dalloc(c.get(), &c->d_clk, 1, L))) return bail(st);
+    if ((st = dalloc(c.get(), &c->d_forces, 3 * MAX_TOOLS, L))) return bail(st);
+    c->scr.forces = c->d_forces;
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_clk, 0, sizeof(DevClock), c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_forces, 0, sizeof(float) * 3 * MAX_TOOLS, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->scr.nnb, 0, sizeof(int) * n, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->scr.pos_half, 0, sizeof(float4) * n, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->scr.nrm, 0, sizeof(float4) * n, c->stream);
+    if (e != cudaSuccess) return bail(fail(MFREE_ERR_CUDA, std::string("alloc_ctx: ") + cudaGetErrorString(e)));
+    out = std::move(c);
+    return MFREE_OK;
+}
+
+// the bytes alloc_ctx + ensure_scratch take (dalloc's max(n, 1) rule included)
+size_t scene_bytes(int n, long long num_cell) {
+    auto b = [](long long k, size_t sz) { return size_t(std::max<long long>(k, 1)) * sz; };
+    const long long hb = (n + HASH_BLOCK - 1) / HASH_BLOCK, fb = (n + 255) / 256;
+    const long long tiles = (num_cell + 1 + SCAN_TILE - 1) / SCAN_TILE;
+    size_t t = 26 * b(n, sizeof(float4)) + b(REC_N * (long long)n, sizeof(float4));
+    t += 3 * b(n, sizeof(int)) + b(hb + 1, sizeof(int)) + b(n, sizeof(int)) + 2 * b(n, sizeof(float4));
+    t += b(fb * 3 * MAX_TOOLS, sizeof(float)) + b(1, sizeof(DevClock)) + b(3 * MAX_TOOLS, sizeof(float));
+    t += b(num_cell + 1, sizeof(int)) + b(num_cell + 2 + SCAN_TILE, sizeof(int)) + b(tiles + 1, sizeof(int));
+    t += single_table_bytes();
+    return t;
+}
+
+int clone_ctx(const mfree_ctx *src, cudaStream_t s, std::unique_ptr<mfree_ctx> &out) {
+    std::unique_ptr<mfree_ctx> c;
+    int st = alloc_ctx(src->n_init, s, c);
+    if (st) return st;
+    c->phys = src->phys;
+    c->corr = src->corr;
+    c->joco = src->joco;
+    c->twp = src->twp;
+    c->ttool = src->ttool;
+    c->opt = src->opt;
+    c->plastic = src->plastic;
+    c->grid_set = src->grid_set;
+    for (int d = 0; d < 3; d++) {
+        c->g_bbmin[d] = src->g_bbmin[d];
+        c->g_bbmax[d] = src->g_bbmax[d];
+        c->g_vel[d] = src->g_vel[d];
+        c->b_min[d] = src->b_min[d];
+        c->b_max[d] = src->b_max[d];
+        c->b_vel[d] = src->b_vel[d];
+    }
+    c->g_dx = src->g_dx;
+    c->nx = src->nx;
+    c->ny = src->ny;
+    c->nz = src->nz;
+    c->num_cell = src->num_cell;
+    c->blank_set = src->blank_set;
+    c->b_vmax = src->b_vmax;
+    c->dt = src->dt;
+    c->t = src->t;
+    c->time_set = src->time_set;
+    c->steps = src->steps;
+    c->cur = src->cur;
+    c->pending = src->pending;
+    for (const auto &t : src->tools) {
+        auto d = std::make_unique<DevTool>(*t);
+        d->d_tri = nullptr;
+        d->d_cells = nullptr;
+        const size_t ntri = size_t(10) * std::max(t->ntri_dev, 1), ncell = t->host.cells.size();
+        CUDA_TRY(cudaMalloc(&d->d_tri, sizeof(float4) * ntri));
+        CUDA_TRY(cudaMalloc(&d->d_cells, sizeof(int) * ncell));
+        CUDA_TRY(cudaMemcpyAsync(d->d_tri, t->d_tri, sizeof(float4) * ntri, cudaMemcpyDeviceToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(d->d_cells, t->d_cells, sizeof(int) * ncell, cudaMemcpyDeviceToDevice, s));
+        c->bytes += sizeof(float4) * ntri + sizeof(int) * ncell;
+        c->tools.push_back(std::move(d));
+    }
+    if ((st = ensure_scratch(c.get()))) return st;
+    const State &A = src->st[src->cur], &B = c->st[src->cur];
+    const float4 *from[] = {A.pos4, A.vel4, A.sa4, A.sb4, A.da4, A.dv4, A.dsa4, A.dsb4, A.fc4, A.ft4, A.bc4, A.lo4, A.lo4b};
+    float4 *to[] = {B.pos4, B.vel4, B.sa4, B.sb4, B.da4, B.dv4, B.dsa4, B.dsb4, B.fc4, B.ft4, B.bc4, B.lo4, B.lo4b};
+    for (int k = 0; k < 13; k++)
+        CUDA_TRY(cudaMemcpyAsync(to[k], from[k], sizeof(float4) * src->n_init, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(c->d_clk, src->d_clk, sizeof(DevClock), cudaMemcpyDeviceToDevice, s));
+    c->clock_dirty = false;
+    out = std::move(c);
+    return MFREE_OK;
+}
+
+}  // namespace host
+}  // namespace mfree
 
 // ======================================================================= ABI
 extern "C" {
@@ -389,47 +511,9 @@ int mfree_create(int n, const float *pos4, const float *vel4, const float *rho, 
                  const float *fixed, const float *tool_p, void *stream, mfree_ctx **out) {
     if (!out || n <= 0 || !pos4 || !vel4 || !rho || !h) return fail(MFREE_ERR_ARG, "mfree_create: bad arguments");
     *out = nullptr;
-    int dev = 0;
-    CUDA_TRY(cudaGetDevice(&dev));
-    auto c = std::make_unique<mfree_ctx>();
-    c->n_init = n;
-    c->stream = (cudaStream_t)stream;
-    if (!c->stream) {  // own stream: graph capture is not allowed on the legacy default stream
-        CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-        c->own_stream = true;
-    }
-    c->device = dev;
-    CUDA_TRY(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev));
-    c->opt.max_secant_iter = 100;
-    auto &L = c->allocs;
-    int st;
-    for (int b = 0; b < 2; b++) {
-        State &S = c->st[b];
-        float4 **f[] = {&S.pos4, &S.vel4, &S.sa4, &S.sb4, &S.da4, &S.dv4, &S.dsa4, &S.dsb4,
-                        &S.fc4, &S.ft4, &S.bc4, &S.lo4, &S.lo4b};
-        for (auto p : f)
-            if ((st = dalloc(c.get(), p, n, L))) return st;
-    }
-    {
-        float4 *base = nullptr;
-        if ((st = dalloc(c.get(), &base, size_t(REC_N) * n, L))) return st;
-        for (int k = 0; k < REC_N; k++) c->rec.f[k] = base + size_t(k) * n;
-    }
-    if ((st = dalloc(c.get(), &c->scr.key, n, L))) return st;
-    if ((st = dalloc(c.get(), &c->scr.key_sorted, n, L))) return st;
-    if ((st = dalloc(c.get(), &c->scr.perm, n, L))) return st;
-    if ((st = dalloc(c.get(), &c->scr.blank_block, (n + HASH_BLOCK - 1) / HASH_BLOCK + 1, L))) return st;
-    if ((st = dalloc(c.get(), &c->scr.nnb, n, L))) return st;
-    if ((st = dalloc(c.get(), &c->scr.pos_half, n, L))) return st;
-    if ((st = dalloc(c.get(), &c->scr.nrm, n, L))) return st;
-    if ((st = dalloc(c.get(), &c->scr.force_part, size_t((n + 255) / 256) * 3 * MAX_TOOLS, L))) return st;
-    if ((st = dalloc(c.get(), &c->d_clk, 1, L))) return st;
-    if ((st = dalloc(c.get(), &c->d_forces, 3 * MAX_TOOLS, L))) return st;
-    CUDA_TRY(cudaMemsetAsync(c->d_clk, 0, sizeof(DevClock), c->stream));
-    CUDA_TRY(cudaMemsetAsync(c->d_forces, 0, sizeof(float) * 3 * MAX_TOOLS, c->stream));
-    CUDA_TRY(cudaMemsetAsync(c->scr.nnb, 0, sizeof(int) * n, c->stream));
-    CUDA_TRY(cudaMemsetAsync(c->scr.pos_half, 0, sizeof(float4) * n, c->stream));
-    CUDA_TRY(cudaMemsetAsync(c->scr.nrm, 0, sizeof(float4) * n, c->stream));
+    std::unique_ptr<mfree_ctx> c;
+    int st = alloc_ctx(n, (cudaStream_t)stream, c);
+    if (st) return st;
     // initial state, reference constructor semantics (zeros except the given fields)
     std::vector<float4> hp(n), hv(n), hz(n, make_float4(0, 0, 0, 0)), hsb(n), hdsb(n), hfc(n), hft(n), hbc(n);
     std::vector<int> perm(n);
@@ -473,6 +557,7 @@ int mfree_create(int n, const float *pos4, const float *vel4, const float *rho, 
 
 int mfree_destroy(mfree_ctx *c) {
     if (!c) return MFREE_OK;
+    if (c->owner) return fail(MFREE_ERR_ARG, "mfree_destroy: the context belongs to a batch (retire it first)");
     cudaStreamSynchronize(c->stream);
     invalidate_graphs(c);
     for (auto &t : c->tools) {
@@ -634,6 +719,7 @@ int mfree_add_tool(mfree_ctx *c, const float *verts, int nv, const int *tris, in
     CUDA_TRY(cudaMalloc(&t->d_tri, sizeof(float4) * h.size()));
     CUDA_TRY(cudaMemcpy(t->d_tri, h.data(), sizeof(float4) * h.size(), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMalloc(&t->d_cells, sizeof(int) * t->host.cells.size()));
+    c->bytes += sizeof(float4) * h.size() + sizeof(int) * t->host.cells.size();
     CUDA_TRY(cudaMemcpy(t->d_cells, t->host.cells.data(), sizeof(int) * t->host.cells.size(), cudaMemcpyHostToDevice));
     c->tools.push_back(std::move(t));
     if (tool_index) *tool_index = int(c->tools.size()) - 1;
@@ -691,28 +777,9 @@ int mfree_get_tool_cells(mfree_ctx *c, int k, int *cells, int *boxed_src) {
     return MFREE_OK;
 }
 
-static int check_empty(mfree_ctx *c, bool wait) {
-    if (!c->nact_pending) return MFREE_OK;
-    if (!wait && cudaEventQuery(c->nact_ev) != cudaSuccess) return MFREE_OK;
-    CUDA_TRY(cudaEventSynchronize(c->nact_ev));
-    c->nact_pending = false;
-    if (*c->h_nact == 0) return fail(MFREE_ERR_EMPTY, "all particles are blanked (outside the blanking box)");
-    return MFREE_OK;
-}
-
-static int note_active_count(mfree_ctx *c) {
-    if (!c->h_nact) {
-        CUDA_TRY(cudaMallocHost(&c->h_nact, sizeof(int)));
-        CUDA_TRY(cudaEventCreateWithFlags(&c->nact_ev, cudaEventDisableTiming));
-    }
-    CUDA_TRY(cudaMemcpyAsync(c->h_nact, &c->d_clk->n_active, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(cudaEventRecord(c->nact_ev, c->stream));
-    c->nact_pending = true;
-    return MFREE_OK;
-}
-
 int mfree_step(mfree_ctx *c, int record_forces) {
     if (!c) return fail(MFREE_ERR_ARG, "null context");
+    if (c->owner) return fail(MFREE_ERR_ARG, "mfree_step: the context belongs to a batch (mfree_batch_step steps it)");
     int st = ready(c);
     if (st) return st;
     if ((st = check_empty(c, false))) return st;
@@ -727,6 +794,7 @@ int mfree_step(mfree_ctx *c, int record_forces) {
 
 int mfree_advance(mfree_ctx *c, int nsteps, int record_every, int use_graph) {
     if (!c || nsteps < 0) return fail(MFREE_ERR_ARG, "bad arguments");
+    if (c->owner) return fail(MFREE_ERR_ARG, "mfree_advance: the context belongs to a batch (mfree_batch_step steps it)");
     int st = ready(c);
     if (st) return st;
     if ((st = check_empty(c, false))) return st;
@@ -741,30 +809,26 @@ int mfree_advance(mfree_ctx *c, int nsteps, int record_every, int use_graph) {
         }
         return MFREE_OK;
     }
-    if (!c->graph_valid || c->graph_record_every != record_every) {
+    if (!c->graph || c->graph_record_every != record_every) {
         invalidate_graphs(c);
-        for (int parity = 0; parity < 2; parity++) {
-            const int keep = c->cur;
-            c->cur = parity;
-            cudaGraph_t g = nullptr;
-            CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-            int e = enqueue_step(c, 2, record_every);
-            cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
-            c->cur = keep;
-            if (e) {
-                if (g) cudaGraphDestroy(g);
-                return e;
-            }
-            if (ce != cudaSuccess) return fail(MFREE_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
-            cudaError_t ie = cudaGraphInstantiate(&c->graph[parity], g, 0);
-            cudaGraphDestroy(g);
-            if (ie != cudaSuccess) return fail(MFREE_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+        // one graph serves both state parities (the parity flips on the device)
+        if ((st = ensure_table(c, record_every))) return st;
+        cudaGraph_t g = nullptr;
+        CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        int e = enqueue_step(c, 2, record_every);
+        cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+        if (e) {
+            if (g) cudaGraphDestroy(g);
+            return e;
         }
-        c->graph_valid = true;
+        if (ce != cudaSuccess) return fail(MFREE_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+        cudaError_t ie = cudaGraphInstantiate(&c->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) return fail(MFREE_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
         c->graph_record_every = record_every;
     }
     for (int k = 0; k < nsteps; k++) {
-        CUDA_TRY(cudaGraphLaunch(c->graph[c->cur], c->stream));
+        CUDA_TRY(cudaGraphLaunch(c->graph, c->stream));
         c->cur ^= 1;
         if (c->pending) c->t = c->t + c->dt;
         c->pending = true;

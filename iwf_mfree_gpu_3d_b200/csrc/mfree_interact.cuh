@@ -1,0 +1,822 @@
+// mfree_interact.cuh -- the pair loop and the fused per-particle rest of the step
+// (kernel templates; mfree_interact.cu instantiates and launches them).
+//
+// Reference path replaced (src/leap_frog.cu:153-171):
+//   do_interactions_monaghan  interactions_gpu.cu:152-471 (CSPM pre-pass, velocity
+//                             gradient, stress divergence with artificial stress,
+//                             artificial viscosity, XSPH, Brookshaw conduction)
+//   do_interactions_heat      interactions_gpu.cu:89-150 (PSE conduction)
+//   do_material_stress_rate_jaumann, do_contmech_continuity/momentum/advection
+//                             actions_gpu.cu:134-300
+//   correct                   leap_frog.cu:72-100
+//   do_plasticity_johnson_cook actions_gpu.cu:371-449
+//   do_reset_contact_forces, do_boundary_conditions(_thermal), do_move_tool_particles
+//                             leap_frog.cu:102-119, actions_gpu.cu:55-68,451-487
+//                             (particles inside a tool box defer these to k_finalize)
+//
+// Work decomposition: a persistent block (512 threads, one per SM) pulls
+// tiles of 4 x 4 x 6 cells from a work counter.  The tile's particles are 16
+// contiguous ranges of the sorted order; the records their 5x5x5 stencils
+// touch are the 64 contiguous column ranges of the 8 x 8 x 10-cell halo,
+// staged into shared memory with one bulk copy per column (TMA
+// cp.async.bulk, completion counted on an mbarrier, bounded waits).  Each
+// target is served by a group of LPP lanes.  Pass A streams the target's
+// candidates (25 column ranges of the staged halo) through the lanes: support
+// test, PSE (which sums every stencil candidate), CSPM matrix, and a ballot
+// that compacts the in-support neighbours into a queue.  Pass B runs the full
+// pair body on the queue only -- the reference evaluates every candidate,
+// ~3.5x more work, and candidates outside the support contribute exact zeros
+// there.  Accumulators are reduced across the group with xor shuffles; then
+// one thread per target runs the per-particle epilogue.
+#pragma once
+
+#include "mfree_kernels.cuh"
+
+namespace mfree {
+
+// 2x2 minors of the column-major (GLM) 3x3 in m[c*3+r]
+__device__ __forceinline__ float det3(const float *m) {
+    auto A = [&](int r, int c) { return m[c * 3 + r]; };
+    return A(0, 0) * (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) - A(1, 0) * (A(0, 1) * A(2, 2) - A(0, 2) * A(2, 1)) +
+           A(2, 0) * (A(0, 1) * A(1, 2) - A(0, 2) * A(1, 1));
+}
+__device__ __forceinline__ void inv3(const float *m, float det, float *o) {
+    auto A = [&](int r, int c) { return m[c * 3 + r]; };
+    const float id = 1.0f / det;
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            // o(r,c) = cofactor(c,r)/det
+            const int r0 = (c + 1) % 3, r1 = (c + 2) % 3, c0 = (r + 1) % 3, c1 = (r + 2) % 3;
+            o[c * 3 + r] = (A(r0, c0) * A(r1, c1) - A(r0, c1) * A(r1, c0)) * id;
+        }
+}
+
+struct IData {
+    float x, y, z, vx, vy, vz, rho, c, h, T, tool;
+    float h1, fac;
+    float s[6];  // sigma_i xx yy zz xy xz yz
+    float R[6];  // R_i
+};
+
+// gradient factor of cubic_spline (kernels.cuh:26-69): value w and
+// dfac = der*fac with grad W = dfac * (x_i - x_j)
+__device__ __forceinline__ void spline(float r2, float h1, float fac, float &w, float &dfac) {
+    const float rinv = rsqrtf(r2);
+    const float r = r2 * rinv;
+    const float q = r * h1;
+    float val, der;
+    if (q > 1.f) {
+        const float t = 2.f - q, t2 = t * t;
+        val = 0.25f * t2 * t;
+        der = -0.75f * t2 * h1 * rinv;
+    } else {
+        val = 1.f - 1.5f * q * q * (1.f - 0.5f * q);
+        der = -3.0f * q * (1.f - 0.75f * q) * h1 * rinv;
+    }
+    w = val * fac;
+    dfac = der * fac;
+}
+
+template <bool CSPM, int COND>
+__device__ __forceinline__ void pair_body(const Params &P, const IData &I, const float *invB, const float4 Pj,
+                                          const float4 Vj, const float4 Aj, const float4 Bj, const float4 Rj,
+                                          const float4 Cj, float *acc) {
+    const float dx = I.x - Pj.x, dy = I.y - Pj.y, dz = I.z - Pj.z;
+    const float r2 = dist2_rn(dx, dy, dz);
+    float w, dfac;
+    spline(r2, I.h1, I.fac, w, dfac);
+    float gx = dfac * dx, gy = dfac * dy, gz = dfac * dz;
+    if (CSPM) {
+        const float ux = gx * invB[0] + gy * invB[3] + gz * invB[6];
+        const float uy = gx * invB[1] + gy * invB[4] + gz * invB[7];
+        const float uz = gx * invB[2] + gy * invB[5] + gz * invB[8];
+        gx = ux; gy = uy; gz = uz;
+    }
+    const bool mech = !(I.tool == 1.f) && !(Pj.w == 1.f);
+    const float volj = Cj.w;
+    if (mech) {
+        const float dvx = Vj.x - I.vx, dvy = Vj.y - I.vy, dvz = Vj.z - I.vz;
+        const float ax = dvx * volj, ay = dvy * volj, az = dvz * volj;
+        acc[0] = fmaf(ax, gx, acc[0]); acc[1] = fmaf(ax, gy, acc[1]); acc[2] = fmaf(ax, gz, acc[2]);
+        acc[3] = fmaf(ay, gx, acc[3]); acc[4] = fmaf(ay, gy, acc[4]); acc[5] = fmaf(ay, gz, acc[5]);
+        acc[6] = fmaf(az, gx, acc[6]); acc[7] = fmaf(az, gy, acc[7]); acc[8] = fmaf(az, gz, acc[8]);
+        float Rxx = 0.f, Ryy = 0.f, Rzz = 0.f, Rxy = 0.f, Rxz = 0.f, Ryz = 0.f;
+        if (P.wdeltap > 0.f) {
+            float fab = w * P.inv_wdeltap;
+            fab *= fab;
+            fab *= fab;
+            Rxx = fab * (I.R[0] + Rj.x);
+            Ryy = fab * (I.R[1] + Rj.y);
+            Rzz = fab * (I.R[2] + Rj.z);
+            Rxy = fab * (I.R[3] + Rj.w);
+            Rxz = fab * (I.R[4] + Cj.x);
+            Ryz = fab * (I.R[5] + Cj.y);
+        }
+        const float txx = I.s[0] + Aj.x + Rxx, tyy = I.s[1] + Aj.y + Ryy, tzz = I.s[2] + Aj.z + Rzz;
+        const float txy = I.s[3] + Aj.w + Rxy, txz = I.s[4] + Bj.x + Rxz, tyz = I.s[5] + Bj.y + Ryz;
+        acc[9] = fmaf(txx, gx, fmaf(txy, gy, fmaf(txz, gz, acc[9])));
+        acc[10] = fmaf(txy, gx, fmaf(tyy, gy, fmaf(tyz, gz, acc[10])));
+        acc[11] = fmaf(txz, gx, fmaf(tyz, gy, fmaf(tzz, gz, acc[11])));
+        const float vr = -(dvx * dx + dvy * dy + dvz * dz);  // (v_i - v_j).(x_i - x_j)
+        const float rhoij = 0.5f * (I.rho + Vj.w);
+        const float irho = __fdividef(1.0f, rhoij);
+        {   // artificial viscosity for approaching pairs (vr < 0), without a branch
+            const float cij = 0.5f * (I.c + Bj.z), hij = 0.5f * (I.h + Bj.w);
+            const float mu = vr < 0.f ? __fdividef(hij * vr, r2 + P.av_eta * P.av_eta * hij * hij) : 0.f;
+            const float pij = (-P.av_alpha * cij * mu + P.av_beta * mu * mu) * irho;
+            acc[12] = fmaf(-pij, gx, acc[12]);
+            acc[13] = fmaf(-pij, gy, acc[13]);
+            acc[14] = fmaf(-pij, gz, acc[14]);
+        }
+        const float xw = w * irho;
+        acc[15] = fmaf(-xw, dvx, acc[15]);  // (w/rho_ij)(v_i - v_j)
+        acc[16] = fmaf(-xw, dvy, acc[16]);
+        acc[17] = fmaf(-xw, dvz, acc[17]);
+    }
+    if (COND == MFREE_COND_BROOKSHAW) {
+        // 2 (m/rho_j)(T_i - T_j) e.grad W / r = 2 V_j (T_i - T_j) (d.grad W)/r^2; factor 2 in the epilogue
+        acc[18] = fmaf(volj * (I.T - Cj.z), __fdividef(dx * gx + dy * gy + dz * gz, r2), acc[18]);
+    }
+}
+
+// ------------------------------------------------------------ epilogue --
+template <bool PREC, int COND>
+__device__ void epilogue(const StepArgs &a, int i, const float *res) {
+    const Params &P = a.p;
+    const State &S = a.b;
+    float4 pos = S.pos4[i], vel = S.vel4[i], sa = S.sa4[i], sb = S.sb4[i];
+    float4 da = S.da4[i], dv = S.dv4[i], dsa = S.dsa4[i], dsb = S.dsb4[i];
+    float4 ft = S.ft4[i], fc = S.fc4[i];
+    float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), lob = lo;
+    if (PREC) {
+        lo = S.lo4[i];
+        lob = S.lo4b[i];
+    }
+    const float dt = P.dt;
+    const HalfStep hs = half_step<PREC>(0.5f * dt, pos, vel, sa, sb, da, dv, dsa, dsb, lo, lob);
+    const float tool_p = fc.w;
+    const bool tool = tool_p == 1.f;
+    const float fixed = dsb.w;
+    // ---- rates
+    float pt[3], vt[3], St[6], rho_t, T_t;
+    if (!tool) {
+        float L[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) L[k] = res[k];
+        jaumann(L, hs.S, P.G, St);
+        rho_t = -hs.rho * (L[0] + L[4] + L[8]);
+        const float im = 1.0f / P.mass;
+        vt[0] = P.mass * (res[12] + res[9]) + fc.x * im + ft.x * im;
+        vt[1] = P.mass * (res[13] + res[10]) + fc.y * im + ft.y * im;
+        vt[2] = P.mass * (res[14] + res[11]) + fc.z * im + ft.z * im;
+        const float xf = -P.xspheps * P.mass;
+        pt[0] = fmaf(xf, res[15], hs.vx);
+        pt[1] = fmaf(xf, res[16], hs.vy);
+        pt[2] = fmaf(xf, res[17], hs.vz);
+    } else {
+        pt[0] = pt[1] = pt[2] = 0.f;
+        vt[0] = vt[1] = vt[2] = 0.f;
+        St[0] = dsa.x; St[1] = dsa.y; St[2] = dsa.z; St[3] = dsa.w; St[4] = dsb.x; St[5] = dsb.y;
+        rho_t = da.w;
+    }
+    T_t = dv.w;
+    if (COND == MFREE_COND_BROOKSHAW) {
+        const float al = tool_p == 0.f ? P.wp_alpha : P.tool_alpha;
+        if (al != 0.f) T_t = al * (2.0f * res[18]);
+    } else if (COND == MFREE_COND_PSE) {
+        if (P.wp_alpha != 0.f) {
+            const float al = tool ? P.tool_alpha : P.wp_alpha;
+            const float h = pos.w, h2 = h * h;
+            const float coef = 4.0f / (h2 * h2 * h * 5.5683279968317078f);  // pi^1.5
+            T_t = al * coef * res[18];
+        }
+    }
+    // ---- corrector x1 = x0 + dt * xdot (leap_frog.cu:72-100)
+    if (PREC) {
+        acc_comp(pos.x, lo.x, dt, pt[0]);
+        acc_comp(pos.y, lo.y, dt, pt[1]);
+        acc_comp(pos.z, lo.z, dt, pt[2]);
+        acc_comp(vel.x, lo.w, dt, vt[0]);
+        acc_comp(vel.y, lob.x, dt, vt[1]);
+        acc_comp(vel.z, lob.y, dt, vt[2]);
+    } else {
+        pos.x = fmaf(dt, pt[0], pos.x);
+        pos.y = fmaf(dt, pt[1], pos.y);
+        pos.z = fmaf(dt, pt[2], pos.z);
+        vel.x = fmaf(dt, vt[0], vel.x);
+        vel.y = fmaf(dt, vt[1], vel.y);
+        vel.z = fmaf(dt, vt[2], vel.z);
+    }
+    float s[6] = {fmaf(dt, St[0], sa.x), fmaf(dt, St[1], sa.y), fmaf(dt, St[2], sa.z),
+                  fmaf(dt, St[3], sa.w), fmaf(dt, St[4], sb.x), fmaf(dt, St[5], sb.y)};
+    vel.w = fmaf(dt, rho_t, vel.w);  // rho
+    float T = fmaf(dt, T_t, sb.z);
+    float eps = sb.w, epsd = dsb.z;
+    // ---- Johnson-Cook radial return (actions_gpu.cu:371-449)
+    if (P.plastic && !tool) {
+        const float nS = sqrtf(s[0] * s[0] + s[1] * s[1] + s[2] * s[2] + 2.f * (s[3] * s[3] + s[5] * s[5] + s[4] * s[4]));
+        float Tc = T;
+        if (P.jc_clamp != 0.f) Tc = Tc > P.jc_Tmelt ? P.jc_Tmelt - 1.f : Tc;
+        const float svm = 1.22474487139158905f * nS;
+        const float sY = jc_sigma_yield(P, eps, epsd, Tc);
+        if (svm < sY) {
+            epsd = 0.f;
+        } else {
+            bool failed = false;
+            const float s23 = 0.81649658092772603f;
+            const float init = fmaxf(epsd * dt * s23, 1e-8f);
+            const float dl = jc_secant(P, init, nS, eps, Tc, dt, failed);
+            if (failed) atomicAdd(&a.clk->secant_failures, 1ull);
+            const float e1 = eps + s23 * fmaxf(dl, 0.f);
+            const float ed1 = s23 * fmaxf(dl, 0.f) / dt;
+            const float f = dl * 2.f * P.G / nS;
+#pragma unroll
+            for (int k = 0; k < 6; k++) s[k] = s[k] - s[k] * f;
+            if (P.wp_tq != 0.f) {
+                const float sY2 = jc_sigma_yield(P, e1, ed1, Tc);
+                T += P.wp_tq / (P.wp_cp * vel.w) * (e1 - eps) * sY2;
+            }
+            eps = e1;
+            epsd = ed1;
+        }
+    }
+    // ---- contact reset; particles inside a tool box finish in k_finalize
+    const bool deferred = !tool && contact_candidate(a, pos.x, pos.y, pos.z);
+    fc.x = fc.y = fc.z = 0.f;  // w keeps tool_p
+    ft.x = ft.y = ft.z = 0.f;  // w keeps blanked
+    if (!deferred) {
+        if (!tool && fixed != 0.f) {
+            const float4 bc = S.bc4[i];
+            vel.x = bc.x; vel.y = bc.y; vel.z = bc.z;
+            if (PREC) { lo.w = 0.f; lob.x = lob.y = 0.f; }
+            pt[0] = pt[1] = pt[2] = 0.f;
+            vt[0] = vt[1] = vt[2] = 0.f;
+        }
+        if (P.thermal && fixed == 1.f) T = P.wp_Tinit;
+        if (P.diagnostics) a.s.nrm[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (tool) {  // do_move_tool_particles
+        if (PREC) {
+            acc_comp(pos.x, lo.x, dt, P.tool0_vel[0]);
+            acc_comp(pos.y, lo.y, dt, P.tool0_vel[1]);
+            acc_comp(pos.z, lo.z, dt, P.tool0_vel[2]);
+        } else {
+            pos.x = fmaf(P.tool0_vel[0], dt, pos.x);
+            pos.y = fmaf(P.tool0_vel[1], dt, pos.y);
+            pos.z = fmaf(P.tool0_vel[2], dt, pos.z);
+        }
+    }
+    S.pos4[i] = pos;
+    S.vel4[i] = vel;
+    S.sa4[i] = make_float4(s[0], s[1], s[2], s[3]);
+    S.sb4[i] = make_float4(s[4], s[5], T, eps);
+    S.da4[i] = make_float4(pt[0], pt[1], pt[2], rho_t);
+    S.dv4[i] = make_float4(vt[0], vt[1], vt[2], T_t);
+    S.dsa4[i] = make_float4(St[0], St[1], St[2], St[3]);
+    S.dsb4[i] = make_float4(St[4], St[5], epsd, fixed);
+    S.fc4[i] = fc;
+    S.ft4[i] = ft;
+    if (PREC) {
+        S.lo4[i] = lo;
+        S.lo4b[i] = lob;
+    }
+    if (P.diagnostics) a.s.nnb[i] = __float_as_int(res[19]);
+}
+
+// ---------------------------------------------------------- pair kernel --
+// Tile = TX x TY x TZ cells of the cell grid; its particles are 16 contiguous
+// column ranges of the sorted order.  Their 5x5x5 stencils lie in the halo of
+// HX x HY x HZ cells: 64 contiguous column ranges of each record array, which
+// one bulk copy per column and array (cp.async.bulk, completion counted on an
+// mbarrier) stages into six shared-memory arrays.  A tile whose halo exceeds
+// the staging capacity reads the same records from global memory instead.
+constexpr int TX = 4, TY = 4;         // the depth (cells along z) is Params::tile_z
+constexpr int HX = TX + 4, HY = TY + 4;
+constexpr int CSROW = TILE_Z_MAX + 5;  // cell starts kept per halo column
+constexpr int NHC = HX * HY;           // halo columns
+constexpr int NTC = TX * TY;           // target columns
+constexpr int TILE_THREADS = 512;
+constexpr int TILE_WARPS = TILE_THREADS / 32;
+constexpr int TCAP = 320;              // targets per pass of a tile
+constexpr int QCAP_T = 96;             // in-support queue per target before the rescan path
+constexpr int SMEM_LIMIT = 232448;     // per-block shared memory of sm_100
+
+template <int LPP> struct TileSmem {
+    static constexpr int G = 32 / LPP;
+    float res[TCAP][NRES + 1];
+    int tgt[TCAP];       // sorted index of each target of the pass
+    int q[TILE_WARPS][G][QCAP_T];
+    int cbase[TILE_WARPS][G][25];
+    int cpref[TILE_WARPS][G][26];
+    int cellstart[NHC][CSROW];
+    int hoff[NHC];       // staged offset of a halo column
+    int hstart[NHC];     // global start of a halo column
+    int hlen[NHC];
+    int tstart[NTC];
+    int tpref[NTC + 1];
+    unsigned long long bar;
+    int tile, total, staged, parity, scene;
+};
+__host__ __device__ constexpr size_t round128(size_t b) { return (b + 127) / 128 * 128; }
+// shared memory: the tables, the scene's arguments, the staged records
+template <int LPP> __host__ __device__ constexpr size_t args_offset() { return round128(sizeof(TileSmem<LPP>)); }
+template <int LPP> __host__ __device__ constexpr size_t rec_offset() {
+    return args_offset<LPP>() + round128(sizeof(StepArgs));
+}
+template <int LPP> __host__ __device__ constexpr int rec_capacity() {
+    return int((SMEM_LIMIT - rec_offset<LPP>()) / (REC_N * sizeof(float4)));
+}
+__host__ __device__ inline int tile_count(const Params &P) {
+    return ((P.gnx + TX - 1) / TX) * ((P.gny + TY - 1) / TY) * ((P.gnz + P.tile_z - 1) / P.tile_z);
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return unsigned(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ void mbar_init(unsigned long long *b, unsigned n) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(n) : "memory");
+}
+__device__ __forceinline__ void mbar_expect(unsigned long long *b, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(unsigned long long *b, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void bulk_to_smem(void *dst, const void *src, unsigned bytes, unsigned long long *b) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(b))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// inclusive scan over the LPP lanes of a group
+template <int LPP> __device__ __forceinline__ int group_scan(int v, int sl) {
+#pragma unroll
+    for (int o = 1; o < LPP; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, v, o, LPP);
+        if (sl >= o) v += y;
+    }
+    return v;
+}
+
+// one target: stencil ranges, pass A (support, PSE, queue), CSPM pass over
+// the queue, pair pass over the queue, group reduction
+template <int LPP, bool CSPM, int COND, bool STAGED, class SM>
+__device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const float4 *RF, int rstride,
+                                               int i, bool valid, int tt, int warp, int g, int sl, int lane, int X0,
+                                               int Y0, int zl) {
+    const Params &P = a.p;
+    const int nx = P.gnx, ny = P.gny, nz = P.gnz;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const unsigned gmask = LPP == 32 ? 0xffffffffu : (((1u << LPP) - 1u) << (g * LPP));
+    // the six record arrays at RF + k * rstride (shared memory or global)
+    const float4 *__restrict__ rP = RF + REC_P * rstride;
+    const float4 *__restrict__ rV = RF + REC_V * rstride;
+    const float4 *__restrict__ rA = RF + REC_A * rstride;
+    const float4 *__restrict__ rB = RF + REC_B * rstride;
+    const float4 *__restrict__ rR = RF + REC_R * rstride;
+    const float4 *__restrict__ rC = RF + REC_C * rstride;
+    // the target's cell; its own records come from the staged halo (its cell
+    // column is one of the halo's) or from global memory
+    const unsigned key = a.s.key_sorted[i];
+    const int nyz = ny * nz;
+    const int gi = int(key) / nyz, rem = int(key) - gi * nyz, gj = rem / nz, gk = rem - gj * nz;
+    IData I;
+    {
+        int si = i;
+        if (STAGED) {
+            const int lc = (gi - X0 + 2) * HY + (gj - Y0 + 2);
+            si = sm.hoff[lc] + (i - sm.hstart[lc]);
+        }
+        const float4 Pi = rP[si], Vi = rV[si], Ai = rA[si], Bi = rB[si], Ri = rR[si], Ci = rC[si];
+        I.x = Pi.x; I.y = Pi.y; I.z = Pi.z; I.tool = Pi.w;
+        I.vx = Vi.x; I.vy = Vi.y; I.vz = Vi.z; I.rho = Vi.w;
+        I.s[0] = Ai.x; I.s[1] = Ai.y; I.s[2] = Ai.z; I.s[3] = Ai.w; I.s[4] = Bi.x; I.s[5] = Bi.y;
+        I.c = Bi.z; I.h = Bi.w;
+        I.R[0] = Ri.x; I.R[1] = Ri.y; I.R[2] = Ri.z; I.R[3] = Ri.w; I.R[4] = Ci.x; I.R[5] = Ci.y;
+        I.T = Ci.z;
+        I.h1 = 1.0f / I.h;
+        I.fac = 0.31830988618379067f * I.h1 * I.h1 * I.h1;
+    }
+    int *cb = sm.cbase[warp][g];
+    int *cp = sm.cpref[warp][g];
+    int *qq = sm.q[warp][g];
+    // ---- the 25 stencil columns as ranges of the record arrays, with their prefix
+    {
+        const int klo = max(gk - 2, 0) - zl, khi = min(gk + 2, nz - 1) - zl + 1;
+        constexpr int NSET = (25 + LPP - 1) / LPP;
+        int carry = 0;
+#pragma unroll
+        for (int k = 0; k < NSET; k++) {
+            const int c = sl + k * LPP;
+            int b = 0, l = 0;
+            if (valid && c < 25) {
+                const int cx = gi + c / 5 - 2, cy = gj + c % 5 - 2;
+                if (cx >= 0 && cx < nx && cy >= 0 && cy < ny) {
+                    const int lc = (cx - X0 + 2) * HY + (cy - Y0 + 2);
+                    const int s0 = sm.cellstart[lc][klo];
+                    l = sm.cellstart[lc][khi] - s0;
+                    b = STAGED ? sm.hoff[lc] + (s0 - sm.hstart[lc]) : s0;
+                }
+            }
+            const int inc = group_scan<LPP>(l, sl);
+            if (c < 25) {
+                cb[c] = b;
+                cp[c] = carry + inc - l;
+            }
+            carry += __shfl_sync(0xffffffffu, inc, (g * LPP) + LPP - 1);
+        }
+        if (sl == 0) cp[25] = carry;
+    }
+    __syncwarp();
+    // ---- candidates: lane sl of the group scans the contiguous chunk
+    // [kb, ke) of the flattened stencil (columns in order); the column it is
+    // in and the record index advance in registers
+    const int total = cp[25];
+    const int per = (total + LPP - 1) / LPP;
+    int maxper = per;
+#pragma unroll
+    for (int o = 16; o >= LPP; o >>= 1) maxper = max(maxper, __shfl_xor_sync(0xffffffffu, maxper, o));
+    const int kb = min(sl * per, total), ke = min(kb + per, total);
+    // visits the candidates of the chunk, one per step of the group, and
+    // calls fn(j, active) on every step (active false past the chunk's end)
+    auto scan = [&](auto &&fn) {
+        int col = 0;
+        while (col < 24 && cp[col + 1] <= kb) col++;
+        int cend = cp[col + 1];
+        int j = cb[col] + (kb - cp[col]);
+#pragma unroll 2
+        for (int it = 0; it < maxper; it++) {
+            const int k = kb + it;
+            const bool act = k < ke;
+            if (act) {
+                while (k >= cend) {  // next non-empty column (k < total keeps col <= 24)
+                    col++;
+                    cend = cp[col + 1];
+                    j = cb[col];
+                }
+            }
+            fn(j, act);
+            j++;
+        }
+    };
+    // ---- pass A: support test, PSE, queue
+    const float pse_k = -1.44269504088896341f * I.h1 * I.h1;  // exp(-r^2/h^2) = 2^(pse_k r^2)
+    const float four_h2 = __fmul_rn(__fmul_rn(4.0f, I.h), I.h);
+    int qn = 0, cnt = 0;
+    float pse = 0.f;
+    scan([&](int j, bool act) {
+        bool ins = false;
+        if (act) {
+            const float4 Pj = rP[j];
+            const float dx = I.x - Pj.x, dy = I.y - Pj.y, dz = I.z - Pj.z;
+            const float r2 = dist2_rn(dx, dy, dz);
+            ins = !(r2 >= four_h2) && (r2 > 9.99999994e-9f);  // in_support()
+            if (COND == MFREE_COND_PSE) {
+                const float4 Cj = rC[j];
+                pse = fmaf((Cj.z - I.T) * Cj.w, exp2f(pse_k * r2), pse);
+            }
+        }
+        cnt += ins ? 1 : 0;
+        const unsigned m = __ballot_sync(0xffffffffu, ins) & gmask;
+        if (ins) {
+            const int pos = qn + __popc(m & lt_mask);
+            if (pos < QCAP_T) qq[pos] = j;
+        }
+        qn += __popc(m);
+    });
+    __syncwarp();
+    const int qv = min(qn, QCAP_T);
+    int maxq = qv;
+#pragma unroll
+    for (int o = 16; o >= LPP; o >>= 1) maxq = max(maxq, __shfl_xor_sync(0xffffffffu, maxq, o));
+    const bool overflow = __any_sync(0xffffffffu, qn > QCAP_T);
+    // in-support neighbours beyond the queue: found again by the same scan
+    auto for_overflow = [&](auto &&fn) {
+        int ord = 0;
+        scan([&](int j, bool act) {
+            bool ins = false;
+            if (act && qn > QCAP_T) {
+                const float4 Pj = rP[j];
+                ins = in_support(dist2_rn(I.x - Pj.x, I.y - Pj.y, I.z - Pj.z), I.h);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, ins) & gmask;
+            const int pos = ord + __popc(m & lt_mask);
+            if (ins && pos >= QCAP_T) fn(j);
+            ord += __popc(m);
+        });
+    };
+    // ---- CSPM matrix over the in-support neighbours (interactions_gpu.cu:227-295)
+    float invB[9] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};
+    if (CSPM) {
+        float Bm[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) Bm[k] = 0.f;
+        auto bterm = [&](int j) {
+            const float4 Pj = rP[j];
+            if (I.tool == 1.f || Pj.w == 1.f) return;
+            const float dx = I.x - Pj.x, dy = I.y - Pj.y, dz = I.z - Pj.z;
+            float w, dfac;
+            spline(dist2_rn(dx, dy, dz), I.h1, I.fac, w, dfac);
+            const float vol = -rC[j].w;
+            const float d[3] = {dx, dy, dz};
+            const float gr[3] = {dfac * dx, dfac * dy, dfac * dz};
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int r = 0; r < 3; r++) Bm[c * 3 + r] = fmaf(vol * d[r], gr[c], Bm[c * 3 + r]);
+        };
+        for (int q0 = 0; q0 < maxq; q0 += LPP) {
+            const int q = q0 + sl;
+            if (q < qv) bterm(qq[q]);
+        }
+        if (overflow) for_overflow(bterm);
+#pragma unroll
+        for (int o = LPP / 2; o >= 1; o >>= 1)
+#pragma unroll
+            for (int k = 0; k < 9; k++) Bm[k] += __shfl_xor_sync(0xffffffffu, Bm[k], o);
+        const float det = det3(Bm);
+        if (det > 9.99999994e-9f) inv3(Bm, det, invB);
+    }
+    // ---- pair body over the in-support neighbours
+    float acc[19];
+#pragma unroll
+    for (int k = 0; k < 19; k++) acc[k] = 0.f;
+    auto pterm = [&](int j) { pair_body<CSPM, COND>(P, I, invB, rP[j], rV[j], rA[j], rB[j], rR[j], rC[j], acc); };
+    for (int q0 = 0; q0 < maxq; q0 += LPP) {
+        const int q = q0 + sl;
+        if (q < qv) pterm(qq[q]);
+    }
+    if (overflow) for_overflow(pterm);
+    if (COND == MFREE_COND_PSE) acc[18] = pse;
+#pragma unroll
+    for (int o = LPP / 2; o >= 1; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 19; k++) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    }
+    if (sl == 0 && valid) {
+        float *rs = sm.res[tt];
+#pragma unroll
+        for (int k = 0; k < 19; k++) rs[k] = acc[k];
+        rs[19] = __int_as_float(cnt);
+    }
+    __syncwarp();
+}
+
+// one tile of the cell grid: target ranges (an empty tile ends there), halo
+// cell starts, staging, then the targets in passes of TCAP.  Returns false
+// when a staging wait ran out (the caller leaves the kernel).
+template <int LPP, bool CSPM, int COND, bool PREC, int CAP>
+__device__ __forceinline__ bool interact_tile(const StepArgs &a, TileSmem<LPP> &sm, float4 *sarr, int tile) {
+    constexpr int G = 32 / LPP;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane / LPP, sl = lane - g * LPP;
+    const Params &P = a.p;
+    const int nx = P.gnx, ny = P.gny, nz = P.gnz;
+    const int TZ = P.tile_z;
+    const int nty = (ny + TY - 1) / TY, ntz = (nz + TZ - 1) / TZ;
+    const int *__restrict__ first = a.s.first;
+    const float4 *gbase = a.r.f[0];  // the record arrays are one allocation: f[k] = f[0] + k * n_init
+    const int gstride = P.n_init;
+    {
+        const int tz = tile % ntz, txy = tile / ntz, ty = txy % nty, tx = txy / nty;
+        const int X0 = tx * TX, Y0 = ty * TY, Z0 = tz * TZ;
+        const int zl = max(Z0 - 2, 0), zh = min(Z0 + TZ + 1, nz - 1);
+        const int nzr = zh - zl + 2;  // cell starts per halo column (inclusive end)
+        // ---- target column ranges first: empty tiles end here
+        if (threadIdx.x < 32) {
+            const int c = threadIdx.x;
+            int s0 = 0, len = 0;
+            if (c < NTC) {
+                const int cx = X0 + c / TY, cy = Y0 + c % TY;
+                if (cx < nx && cy < ny && Z0 < nz) {
+                    const int cb = (cx * ny + cy) * nz;
+                    s0 = first[cb + Z0];
+                    len = first[cb + min(Z0 + TZ - 1, nz - 1) + 1] - s0;
+                }
+                sm.tstart[c] = s0;
+            }
+            const int ti = group_scan<32>(len, c);
+            if (c < NTC) sm.tpref[c] = ti - len;
+            if (c == 31) sm.tpref[NTC] = ti;
+        }
+        __syncthreads();
+        if (sm.tpref[NTC] == 0) return true;  // (the caller's loop head synchronises before the next tile)
+        // ---- halo cell starts
+        for (int e = threadIdx.x; e < NHC * CSROW; e += TILE_THREADS) {
+            const int c = e / CSROW, k = e - c * CSROW;
+            const int cx = X0 - 2 + c / HY, cy = Y0 - 2 + c % HY;
+            int v = 0;
+            if (k < nzr && cx >= 0 && cx < nx && cy >= 0 && cy < ny) v = first[(cx * ny + cy) * nz + zl + k];
+            sm.cellstart[c][k] = v;
+        }
+        __syncthreads();
+        if (warp == 0) {  // prefix sum of the 64 halo columns; staging decision
+            int len2[2];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int c = lane + 32 * h;
+                const int cx = X0 - 2 + c / HY, cy = Y0 - 2 + c % HY;
+                const bool in = cx >= 0 && cx < nx && cy >= 0 && cy < ny;
+                len2[h] = in ? sm.cellstart[c][nzr - 1] - sm.cellstart[c][0] : 0;
+                sm.hstart[c] = sm.cellstart[c][0];
+                sm.hlen[c] = len2[h];
+            }
+            const int i0 = group_scan<32>(len2[0], lane);
+            const int t0 = __shfl_sync(0xffffffffu, i0, 31);
+            const int i1 = group_scan<32>(len2[1], lane);
+            sm.hoff[lane] = i0 - len2[0];
+            sm.hoff[lane + 32] = t0 + i1 - len2[1];
+            const int tot = t0 + __shfl_sync(0xffffffffu, i1, 31);
+            if (lane == 0) {
+                sm.total = tot;
+                sm.staged = tot <= CAP ? 1 : 0;
+                if (sm.staged && tot > 0) mbar_expect(&sm.bar, unsigned(tot) * unsigned(REC_N * sizeof(float4)));
+            }
+        }
+        __syncthreads();
+        const int T = sm.tpref[NTC];
+        const bool staged = sm.staged != 0;
+        if (staged && sm.total > 0) {
+            if (threadIdx.x < REC_N * NHC) {
+                const int k = threadIdx.x / NHC, c = threadIdx.x - k * NHC;
+                const int len = sm.hlen[c];
+                if (len > 0)
+                    bulk_to_smem(sarr + k * CAP + sm.hoff[c], gbase + size_t(k) * gstride + sm.hstart[c],
+                                 unsigned(len) * unsigned(sizeof(float4)), &sm.bar);
+            }
+            const unsigned par = unsigned(sm.parity);
+            unsigned it = 0;
+            bool ok = true;
+            while (!mbar_try(&sm.bar, par)) {
+                if (++it > (1u << 22)) {
+                    ok = false;
+                    break;
+                }
+            }
+            if (!__syncthreads_and(ok)) {
+                // the copies did not complete in time: record it, wait once more
+                // (bounded) for them to land, and leave the kernel
+                if (threadIdx.x == 0) atomicAdd(&a.clk->tile_error, 1);
+                unsigned it2 = 0;
+                while (!mbar_try(&sm.bar, par) && ++it2 < (1u << 22)) {
+                }
+                return false;
+            }
+            if (threadIdx.x == 0) sm.parity ^= 1;
+        }
+        // ---- targets, TCAP per pass
+        for (int t0 = 0; t0 < T; t0 += TCAP) {
+            const int tn = min(TCAP, T - t0);
+            for (int tt = threadIdx.x; tt < tn; tt += TILE_THREADS) {
+                const int tg = t0 + tt;
+                int c = 0;
+                while (c < NTC - 1 && sm.tpref[c + 1] <= tg) c++;
+                sm.tgt[tt] = sm.tstart[c] + (tg - sm.tpref[c]);
+            }
+            __syncthreads();
+            // rounds of TILE_WARPS * G targets; a last round with few targets
+            // left uses more lanes per target so fewer warps idle at the barrier
+            int done = 0;
+#pragma unroll 1
+            while (done < tn) {
+                const int rem = tn - done;
+                if (LPP < 32 && rem <= TILE_WARPS) {
+                    const int tt = done + warp;
+                    const bool valid = tt < tn;
+                    const int i = sm.tgt[valid ? tt : 0];
+                    if (staged)
+                        process_target<32, CSPM, COND, true>(a, sm, sarr, CAP, i, valid, tt, warp, 0, lane, lane, X0,
+                                                             Y0, zl);
+                    else
+                        process_target<32, CSPM, COND, false>(a, sm, gbase, gstride, i, valid, tt, warp, 0, lane, lane,
+                                                              X0, Y0, zl);
+                    done += TILE_WARPS;
+                } else if (LPP < 16 && rem <= 2 * TILE_WARPS) {
+                    const int g2 = lane >> 4, sl2 = lane & 15;
+                    const int tt = done + warp * 2 + g2;
+                    const bool valid = tt < tn;
+                    const int i = sm.tgt[valid ? tt : 0];
+                    if (staged)
+                        process_target<16, CSPM, COND, true>(a, sm, sarr, CAP, i, valid, tt, warp, g2, sl2, lane, X0,
+                                                             Y0, zl);
+                    else
+                        process_target<16, CSPM, COND, false>(a, sm, gbase, gstride, i, valid, tt, warp, g2, sl2, lane,
+                                                              X0, Y0, zl);
+                    done += 2 * TILE_WARPS;
+                } else {
+                    const int tt = done + warp * G + g;
+                    const bool valid = tt < tn;
+                    const int i = sm.tgt[valid ? tt : 0];
+                    if (staged)
+                        process_target<LPP, CSPM, COND, true>(a, sm, sarr, CAP, i, valid, tt, warp, g, sl, lane, X0,
+                                                              Y0, zl);
+                    else
+                        process_target<LPP, CSPM, COND, false>(a, sm, gbase, gstride, i, valid, tt, warp, g, sl, lane,
+                                                               X0, Y0, zl);
+                    done += TILE_WARPS * G;
+                }
+            }
+            // the rounds were the last generic reads of the staged halo: order
+            // them before the next tile's bulk writes (the barriers that follow
+            // carry the order to the threads that issue the copies)
+            fence_proxy_async();
+            __syncthreads();
+            // ---- per-particle rest of the step, one thread per target
+            for (int tt = threadIdx.x; tt < tn; tt += TILE_THREADS) epilogue<PREC, COND>(a, sm.tgt[tt], sm.res[tt]);
+            __syncthreads();
+        }
+    }
+    return true;
+}
+
+template <int LPP> __device__ __forceinline__ void init_tile_smem(TileSmem<LPP> &sm) {
+    if (threadIdx.x == 0) {
+        mbar_init(&sm.bar, 1);
+        sm.parity = 0;
+    }
+    fence_proxy_async();
+    __syncthreads();
+}
+
+// persistent (one block per SM) over the tiles of every scene of the table
+// (one queue); a block copies a scene's arguments into shared memory when its
+// next tile belongs to another scene than its last one
+template <int LPP, bool CSPM, int COND, bool PREC>
+__global__ void __launch_bounds__(TILE_THREADS, 1) kb_interact(BatchTable T) {
+    constexpr int CAP = rec_capacity<LPP>();
+    extern __shared__ __align__(128) unsigned char dyn[];
+    TileSmem<LPP> &sm = *reinterpret_cast<TileSmem<LPP> *>(dyn);
+    StepArgs &sa = *reinterpret_cast<StepArgs *>(dyn + args_offset<LPP>());
+    float4 *sarr = reinterpret_cast<float4 *>(dyn + rec_offset<LPP>());
+    init_tile_smem<LPP>(sm);
+    const int total = T.itile[T.nscenes];
+    int cur = -1;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int t = atomicAdd(T.tile_next, 1);
+            sm.tile = t;
+            sm.scene = t < total ? find_scene(T.itile, T.nscenes, t) : -1;
+        }
+        __syncthreads();
+        const int tile = sm.tile;
+        if (tile >= total) break;
+        const int s = sm.scene;
+        if (s != cur) {  // every thread has finished the last tile (barriers at its end)
+            load_scene_args(sa, T, s);
+            __syncthreads();
+            cur = s;
+        }
+        if (!interact_tile<LPP, CSPM, COND, PREC, CAP>(sa, sm, sarr, tile - T.itile[s])) return;
+    }
+}
+
+// ------------------------------------------------------------ dispatch --
+template <int LPP, bool CSPM, int COND, bool PREC> struct Variant {
+    static cudaError_t batch(const BatchTable &T, int grid, cudaStream_t s) {
+        auto kern = kb_interact<LPP, CSPM, COND, PREC>;
+        if (grid <= 0)  // prepare only: raise the shared-memory limit (outside any graph capture)
+            return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT);
+        kern<<<grid, TILE_THREADS, SMEM_LIMIT, s>>>(T);
+        return cudaGetLastError();
+    }
+};
+
+// calls fn(Variant<LPP, ...>{}) for the variant of the options
+template <int LPP, class F> static cudaError_t with_variant(bool cspm, int cond, bool prec, F &&fn) {
+#define MFREE_CASE(C, CO, PR) \
+    if (cspm == C && cond == CO && prec == PR) return fn(Variant<LPP, C, CO, PR>{});
+    MFREE_CASE(false, MFREE_COND_NONE, false)
+    MFREE_CASE(false, MFREE_COND_BROOKSHAW, false)
+    MFREE_CASE(false, MFREE_COND_PSE, false)
+    MFREE_CASE(true, MFREE_COND_NONE, false)
+    MFREE_CASE(true, MFREE_COND_BROOKSHAW, false)
+    MFREE_CASE(true, MFREE_COND_PSE, false)
+    MFREE_CASE(false, MFREE_COND_NONE, true)
+    MFREE_CASE(false, MFREE_COND_BROOKSHAW, true)
+    MFREE_CASE(false, MFREE_COND_PSE, true)
+    MFREE_CASE(true, MFREE_COND_NONE, true)
+    MFREE_CASE(true, MFREE_COND_BROOKSHAW, true)
+    MFREE_CASE(true, MFREE_COND_PSE, true)
+#undef MFREE_CASE
+    return cudaErrorInvalidValue;
+}
+
+template <class F> static cudaError_t with_lpp(int lpp, bool cspm, int cond, bool prec, F &&fn) {
+    switch (lpp) {
+        case 8: return with_variant<8>(cspm, cond, prec, fn);
+        case 16: return with_variant<16>(cspm, cond, prec, fn);
+        case 32: return with_variant<32>(cspm, cond, prec, fn);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace mfree

@@ -67,21 +67,67 @@ __device__ __forceinline__ bool contact_candidate(const StepArgs &a, float x, fl
     return in;
 }
 
-__global__ void k_clock(StepArgs a, int record_mode);
-__global__ void k_hash(StepArgs a);
+// ------------------------------------------------------ batched launches --
+// The step's kernels run over a table of scenes: one scene (a context's own
+// one-entry table) or many independent scenes of a batch, one launch per
+// kernel either way, so a scene's arithmetic is the same compiled code alone
+// and in a batch.  Every scene keeps
+// its own state, cell list (a segment of its own) and clock; the table lists
+// each scene's arguments once per state parity and, per kernel family, the
+// first block (or tile) of every scene: block b of a launch belongs to the
+// scene s with prefix[s] <= b < prefix[s + 1].
+struct BatchTable {
+    const StepArgs *args;  // [2 s + parity]
+    const int *pblk;       // particle blocks of 256 threads (hash, scatter, gather, finalize)
+    const int *stile;      // scan tiles of SCAN_TILE cells
+    const int *cblk;       // cell blocks of 256 threads (cell fix-up)
+    const int *itile;      // pair-kernel tiles
+    int nscenes;
+    int *tile_next;        // work queue of the pair kernel (reset by kb_clock)
+};
+
+// scene of block x: the last s with prefix[s] <= x (prefix has nscenes + 1 entries)
+__device__ __forceinline__ int find_scene(const int *__restrict__ prefix, int nscenes, int x) {
+    int lo = 0, hi = nscenes - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= x) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// copies scene s's arguments for the parity of its current step into shared
+// memory; every thread of the block calls it, a barrier must follow
+__device__ __forceinline__ void load_scene_args(StepArgs &dst, const BatchTable &T, int s) {
+    const StepArgs *a0 = T.args + 2 * s;
+    const int4 *src = reinterpret_cast<const int4 *>(a0 + (a0->clk->parity & 1));
+    int4 *d = reinterpret_cast<int4 *>(&dst);
+    for (int k = threadIdx.x; k < int(sizeof(StepArgs) / 16); k += blockDim.x) d[k] = src[k];
+}
+
+__global__ void kb_clock(BatchTable T, int record_mode);
+__global__ void kb_hash(BatchTable T);
+__global__ void kb_scan_reduce(BatchTable T);
+__global__ void kb_scan_top(BatchTable T);
+__global__ void kb_scan_down(BatchTable T);
+__global__ void kb_scatter(BatchTable T);
+__global__ void kb_cell_fixup(BatchTable T);
+cudaError_t launch_gather_predict_batch(const BatchTable &T, bool precision, int blocks, cudaStream_t s);
+__global__ void kb_finalize(BatchTable T);
+__global__ void kb_force_final(BatchTable T);
+// one pair-kernel launch over the tiles of every scene (all scenes share the
+// variant); grid <= 0 only prepares the variant
+cudaError_t launch_interact_batch(const BatchTable &T, int lanes_per_particle, bool cspm, int conduction,
+                                  bool precision, int grid, cudaStream_t s);
+
+// the sort kernels on arguments passed by value, for the allocation-free
+// cell-list build (mfree_static.cu)
 __global__ void k_scan_reduce(StepArgs a);
 __global__ void k_scan_top(StepArgs a, int num_tiles, int num_hash_blocks);
 __global__ void k_scan_down(StepArgs a);
 __global__ void k_scatter(StepArgs a);
 __global__ void k_cell_fixup(StepArgs a);
-cudaError_t launch_gather_predict(const StepArgs &a, int blocks, cudaStream_t s);
-__global__ void k_finalize(StepArgs a);
-__global__ void k_force_final(StepArgs a, int num_blocks, float *out);
-
-// launches the pair kernel for the configured variant (mfree_interact.cu);
-// grid <= 0 only prepares the variant (shared-memory attribute)
-cudaError_t launch_interact(const StepArgs &a, int lanes_per_particle, int grid, cudaStream_t s);
-int interact_grid_size(int lanes_per_particle, int n_init, int num_sms);
 
 // message returned by mfree_last_error() (mfree_host.cu)
 void set_last_error(const std::string &msg);

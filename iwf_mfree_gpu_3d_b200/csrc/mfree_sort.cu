@@ -24,14 +24,25 @@
 namespace mfree {
 
 // ----------------------------------------------------------------- clock --
+// batched kernels: block b of the launch is block b - prefix[s] of scene s,
+// whose arguments the block first copies into shared memory
+template <class F> __device__ __forceinline__ void run_batched(const BatchTable &T, const int *prefix, F &&body) {
+    __shared__ StepArgs sa;
+    const int s = find_scene(prefix, T.nscenes, blockIdx.x);
+    load_scene_args(sa, T, s);
+    __syncthreads();
+    body(sa, int(blockIdx.x) - prefix[s]);
+}
+
 // record_mode: 0 no, 1 yes, 2 every Params::record_every steps
-__global__ void k_clock(StepArgs a, int record_mode) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void clock_body(const StepArgs &a, int record_mode) {
     DevClock *c = a.clk;
     const Params &P = a.p;
-    if (c->pending) c->t = c->t + P.dt;  // main(): global_time_current += dt after each iteration
+    if (c->pending) {
+        c->t = c->t + P.dt;  // main(): global_time_current += dt after each iteration
+        c->parity ^= 1;      // the last step's output is this step's input
+    }
     c->pending = 1;
-    c->tile_next = 0;
     const float t = c->t;
     c->record = record_mode == 1 ? 1
                 : record_mode == 2 ? (P.record_every > 0 && (c->step_index % P.record_every) == 0)
@@ -53,10 +64,17 @@ __global__ void k_clock(StepArgs a, int record_mode) {
     }
 }
 
+// one thread per scene; thread 0 also resets the batch's pair-kernel queue
+__global__ void kb_clock(BatchTable T, int record_mode) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s == 0) *T.tile_next = 0;
+    if (s < T.nscenes) clock_body(T.args[2 * s], record_mode);
+}
+
 // ------------------------------------------------- blanking + cell hash --
-__global__ void __launch_bounds__(HASH_BLOCK) k_hash(StepArgs a) {
+__device__ __forceinline__ void hash_body(const StepArgs &a, int bid) {
     const Params &P = a.p;
-    const int i = blockIdx.x * HASH_BLOCK + threadIdx.x;
+    const int i = bid * HASH_BLOCK + threadIdx.x;
     int blank = 0;
     if (i < P.n_init) {
         float4 p = a.a.pos4[i];
@@ -110,7 +128,10 @@ __global__ void __launch_bounds__(HASH_BLOCK) k_hash(StepArgs a) {
         else blank = 1;
     }
     int nb = __syncthreads_count(blank);
-    if (threadIdx.x == 0) a.s.blank_block[blockIdx.x] = nb;
+    if (threadIdx.x == 0) a.s.blank_block[bid] = nb;
+}
+__global__ void __launch_bounds__(HASH_BLOCK) kb_hash(BatchTable T) {
+    run_batched(T, T.pblk, [](const StepArgs &a, int b) { hash_body(a, b); });
 }
 
 // ------------------------------------------------------------- the scan --
@@ -141,10 +162,10 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *warp_sums, int &
     return pre + x - v;
 }
 
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(StepArgs a) {
+__device__ __forceinline__ void scan_reduce_body(const StepArgs &a, int bid) {
     __shared__ int ws[32];
     const int nc = a.p.num_cell;
-    const int base = blockIdx.x * SCAN_TILE;
+    const int base = bid * SCAN_TILE;
     int s = 0;
 #pragma unroll
     for (int k = 0; k < SCAN_ITEMS; k++) {
@@ -153,11 +174,15 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(StepArgs a) {
     }
     int total;
     block_exclusive_scan(s, ws, total);
-    if (threadIdx.x == 0) a.s.tile_sum[blockIdx.x] = total;
+    if (threadIdx.x == 0) a.s.tile_sum[bid] = total;
+}
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(StepArgs a) { scan_reduce_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(SCAN_THREADS) kb_scan_reduce(BatchTable T) {
+    run_batched(T, T.stile, [](const StepArgs &a, int b) { scan_reduce_body(a, b); });
 }
 
 // one block: exclusive scans of the tile sums and of the blanked-per-block counts
-__global__ void __launch_bounds__(1024) k_scan_top(StepArgs a, int num_tiles, int num_hash_blocks) {
+__device__ __forceinline__ void scan_top_body(const StepArgs &a, int num_tiles, int num_hash_blocks) {
     __shared__ int ws[32];
     __shared__ int carry;
     for (int pass = 0; pass < 2; pass++) {
@@ -180,11 +205,23 @@ __global__ void __launch_bounds__(1024) k_scan_top(StepArgs a, int num_tiles, in
         __syncthreads();
     }
 }
+__global__ void __launch_bounds__(1024) k_scan_top(StepArgs a, int num_tiles, int num_hash_blocks) {
+    scan_top_body(a, num_tiles, num_hash_blocks);
+}
+// one block per scene
+__global__ void __launch_bounds__(1024) kb_scan_top(BatchTable T) {
+    __shared__ StepArgs sa;
+    load_scene_args(sa, T, blockIdx.x);
+    __syncthreads();
+    const int tiles = (sa.p.num_cell + 1 + SCAN_TILE - 1) / SCAN_TILE;
+    const int hb = (sa.p.n_init + HASH_BLOCK - 1) / HASH_BLOCK;
+    scan_top_body(sa, tiles, hb);
+}
 
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(StepArgs a) {
+__device__ __forceinline__ void scan_down_body(const StepArgs &a, int bid) {
     __shared__ int ws[32];
     const int nc = a.p.num_cell;
-    const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    const int base = bid * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
     int v[SCAN_ITEMS];
     int s = 0;
 #pragma unroll
@@ -194,7 +231,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(StepArgs a) {
         s += v[k];
     }
     int total;
-    int ex = block_exclusive_scan(s, ws, total) + a.s.tile_sum[blockIdx.x];
+    int ex = block_exclusive_scan(s, ws, total) + a.s.tile_sum[bid];
 #pragma unroll
     for (int k = 0; k < SCAN_ITEMS; k++) {
         int c = base + k;
@@ -202,12 +239,16 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(StepArgs a) {
         ex += v[k];
     }
 }
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(StepArgs a) { scan_down_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(SCAN_THREADS) kb_scan_down(BatchTable T) {
+    run_batched(T, T.stile, [](const StepArgs &a, int b) { scan_down_body(a, b); });
+}
 
 // ---------------------------------------------------------- the scatter --
-__global__ void __launch_bounds__(HASH_BLOCK) k_scatter(StepArgs a) {
+__device__ __forceinline__ void scatter_body(const StepArgs &a, int bid) {
     __shared__ int ws[32];
     const Params &P = a.p;
-    const int i = blockIdx.x * HASH_BLOCK + threadIdx.x;
+    const int i = bid * HASH_BLOCK + threadIdx.x;
     const int N = a.clk->n_active;
     unsigned key = i < P.n_init ? a.s.key[i] : 0u;
     int blank = (i < P.n_init && key >= unsigned(P.num_cell)) ? 1 : 0;
@@ -218,13 +259,17 @@ __global__ void __launch_bounds__(HASH_BLOCK) k_scatter(StepArgs a) {
         int old = atomicSub(&a.s.count[key], 1);  // leaves count[] zero for the next step
         a.s.perm[a.s.first[key] + old - 1] = i;
     } else {
-        a.s.perm[N + a.s.blank_block[blockIdx.x] + rank] = i;
+        a.s.perm[N + a.s.blank_block[bid] + rank] = i;
     }
+}
+__global__ void __launch_bounds__(HASH_BLOCK) k_scatter(StepArgs a) { scatter_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(HASH_BLOCK) kb_scatter(BatchTable T) {
+    run_batched(T, T.pblk, [](const StepArgs &a, int b) { scatter_body(a, b); });
 }
 
 // order each cell's entries by previous index (stable within the cell)
-__global__ void k_cell_fixup(StepArgs a) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void cell_fixup_body(const StepArgs &a, int bid) {
+    const int c = bid * 256 + threadIdx.x;
     if (c >= a.p.num_cell) return;
     const int s = a.s.first[c], e = a.s.first[c + 1];
     if (e - s < 2) return;
@@ -239,12 +284,15 @@ __global__ void k_cell_fixup(StepArgs a) {
         p[m + 1] = v;
     }
 }
+__global__ void __launch_bounds__(256) k_cell_fixup(StepArgs a) { cell_fixup_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(256) kb_cell_fixup(BatchTable T) {
+    run_batched(T, T.cblk, [](const StepArgs &a, int b) { cell_fixup_body(a, b); });
+}
 
 // --------------------------------------------- gather + predictor + EOS --
-template <bool PREC>
-__global__ void __launch_bounds__(256) k_gather_predict(StepArgs a) {
+template <bool PREC> __device__ __forceinline__ void gather_predict_body(const StepArgs &a, int bid) {
     const Params &P = a.p;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = bid * 256 + threadIdx.x;
     if (i >= P.n_init) return;
     const int N = a.clk->n_active;
     int src = a.s.perm[i];
@@ -288,10 +336,13 @@ __global__ void __launch_bounds__(256) k_gather_predict(StepArgs a) {
     r.f[REC_C][i] = make_float4(Rr[4], Rr[5], hs.T, P.mass / hs.rho);
     if (P.diagnostics) a.s.pos_half[i] = make_float4(hs.x, hs.y, hs.z, 0.f);
 }
+template <bool PREC> __global__ void __launch_bounds__(256) kb_gather_predict(BatchTable T) {
+    run_batched(T, T.pblk, [](const StepArgs &a, int b) { gather_predict_body<PREC>(a, b); });
+}
 
-cudaError_t launch_gather_predict(const StepArgs &a, int blocks, cudaStream_t s) {
-    if (a.p.precision) k_gather_predict<true><<<blocks, 256, 0, s>>>(a);
-    else k_gather_predict<false><<<blocks, 256, 0, s>>>(a);
+cudaError_t launch_gather_predict_batch(const BatchTable &T, bool precision, int blocks, cudaStream_t s) {
+    if (precision) kb_gather_predict<true><<<blocks, 256, 0, s>>>(T);
+    else kb_gather_predict<false><<<blocks, 256, 0, s>>>(T);
     return cudaGetLastError();
 }
 

@@ -11,7 +11,10 @@ This module builds the same kind of scene with seeded, deterministic inputs:
   * ``orthogonal_cutting(nx, ny, nz, ...)``: a steel block cut by a 12-triangle
     wedge (0 deg rake, 7 deg clearance) at the +x face -- the 8k and 1M
     workloads;
-  * ``single_grain(...)``: a block cut by a truncated icosphere grain.
+  * ``single_grain(...)``: a block cut by a truncated icosphere grain;
+  * ``mixed_specs(count, seed, ...)`` / ``mixed_scene(spec)``: the uneven
+    scenes of the batched and served workloads (sizes log-uniform, cutting
+    speed, depth, rake and Johnson-Cook A, B, n drawn per scene).
 
 The scene is plain numpy data; the CUDA path (``api.Simulation``) and the CPU
 oracle consume the same arrays.
@@ -300,3 +303,50 @@ def single_grain(nx: int = 400, ny: int = 160, nz: int = 64, dx: float = 1.0e-3,
     sc.grid_bbmin = sc.blank_bbmin = lo.astype(np.float32)
     sc.grid_bbmax = sc.blank_bbmax = hi.astype(np.float32)
     return sc
+
+
+# ---------------------------------------------------- mixed-size workloads --
+
+@dataclasses.dataclass
+class MixedSpec:
+    """One scene of a mixed workload: lattice nx = 4 nz, ny = 2 nz (n = 8 nz^3)."""
+    nz: int
+    v_tool: float       # cm/us
+    depth: float        # in dx
+    rake_deg: float
+    jc_scale: tuple     # factors on Johnson-Cook A, B, n
+    seed: int
+    steps: int = 0      # steps a served request asks for
+
+    @property
+    def n(self) -> int:
+        return 8 * self.nz ** 3
+
+
+def mixed_specs(count: int, seed: int = 1, n_lo: int = 5000, n_hi: int = 200000, steps_lo: int = 0,
+                steps_hi: int = 0) -> List[MixedSpec]:
+    """Scenes with particle counts log-uniform in [n_lo, n_hi] (nz = round((n/8)^(1/3))),
+    v ~ U[1e-4, 5e-3] cm/us (1-50 m/s), depth ~ U[2, 10] dx, rake ~ U[-20, 10] deg,
+    Johnson-Cook A, B, n each x U[0.9, 1.1]; steps ~ U[steps_lo, steps_hi] when given."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for k in range(count):
+        n = math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))
+        nz = max(4, int(round((n / 8.0) ** (1.0 / 3.0))))
+        v = float(rng.uniform(1.0e-4, 5.0e-3))
+        depth = float(rng.uniform(2.0, 10.0))
+        rake = float(rng.uniform(-20.0, 10.0))
+        jc = tuple(float(x) for x in rng.uniform(0.9, 1.1, size=3))
+        steps = int(rng.integers(steps_lo, steps_hi + 1)) if steps_hi > 0 else 0
+        out.append(MixedSpec(nz=nz, v_tool=v, depth=depth, rake_deg=rake, jc_scale=jc, seed=seed * 100003 + k,
+                             steps=steps))
+    return out
+
+
+def mixed_scene(spec: MixedSpec, precision: int = 1) -> Scene:
+    """The cutting scene of a spec: the 8k scene's physics (Brookshaw, artificial
+    stress, no CSPM) with compensated positions by default."""
+    nz = spec.nz
+    return orthogonal_cutting(4 * nz, 2 * nz, nz, v_tool=spec.v_tool, depth=min(spec.depth, nz - 2.0),
+                              seed=spec.seed, rake_deg=spec.rake_deg, jc_scale=spec.jc_scale, precision=precision,
+                              name=f"mixed_{4 * nz}x{2 * nz}x{nz}")
