@@ -18,6 +18,18 @@ collective): weak scaling, value = all ranks' particle-steps / max rank time.
 --impl reference times the reference's CPU algorithm -- the FP64 oracle
 restatement, OpenMP on every host core -- on the same scene (a bounded
 sub-block of it per step when the full scene would not finish in minutes).
+
+At N = 1 the line also carries the two systems forms, measured live:
+  * "batched": 256 independent cutting scenes of log-uniform size in
+    [5k, 200k] particles (seed 1; speed, depth, rake and Johnson-Cook A, B, n
+    drawn per scene; compensated positions) stepped together -- one launch per
+    kernel, one captured graph per step, autotuned tiling -- against the plain
+    path run scene by scene with the same tiling;
+  * "serving": a Poisson request stream admitted into one resident batch by a
+    150 GB budget, with p50/p99 latency (arrival to result) and throughput;
+    rate, duration, sizes and step counts are scaled down so the run takes
+    seconds (the scaling is stated in the line).
+--no-extras skips both.
 """
 from __future__ import annotations
 
@@ -61,6 +73,14 @@ def parse():
     ap.add_argument("--workload", choices=["1m", "8k"], default="1m")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lpp", type=int, default=0, help="lanes per particle (0 = default)")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving measurements")
+    ap.add_argument("--batch-scenes", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=20)
+    ap.add_argument("--serve-rate", type=float, default=4.0, help="requests per second")
+    ap.add_argument("--serve-seconds", type=float, default=20.0, help="arrival window")
+    ap.add_argument("--serve-nmax", type=int, default=100000, help="largest request (particles)")
+    ap.add_argument("--serve-steps", type=int, nargs=2, default=[50, 500], help="steps per request, range")
+    ap.add_argument("--serve-chunk", type=int, default=25, help="steps between admissions")
     return ap.parse_args()
 
 
@@ -328,7 +348,71 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
             "counters": counters}
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.workload)
+    if world == 1 and not args.no_extras:
+        line["batched"] = run_batched(args)
+        line["serving"] = run_serve(args, tuple(line["batched"]["tiling"]))
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------ systems forms -----
+def run_batched(args) -> dict:
+    """Mixed-size scenes stepped together against the plain path scene by scene."""
+    from iwf_mfree_gpu_3d_b200 import api, scenes
+    specs = scenes.mixed_specs(args.batch_scenes, seed=1)
+    n_total = sum(sp.n for sp in specs)
+    K = args.batch_steps
+    b = api.Batch()
+    t0 = time.perf_counter()
+    for sp in specs:
+        b.admit(api.Simulation.from_scene(scenes.mixed_scene(sp)))
+    setup_s = time.perf_counter() - t0
+    lpp, depth, _ = b.autotune(trial_steps=2)
+    b.step(max(args.warmup, 3), use_graph=True)
+    b.sync()
+    b.timer_start()
+    b.step(K, use_graph=True)
+    ms = b.timer_stop()
+    mem = b.info()["bytes"]
+    b.close()
+    # the plain path, one scene after the other, same tiling, same steps
+    plain_ms = 0.0
+    for sp in specs:
+        sim = api.Simulation.from_scene(scenes.mixed_scene(sp), lanes_per_particle=lpp, tile_depth=depth)
+        sim.advance(max(args.warmup, 3), use_graph=True)
+        sim.sync()
+        sim.timer_start()
+        sim.advance(K, use_graph=True)
+        plain_ms += sim.timer_stop()
+        sim.close()
+    batched = n_total * K / (ms * 1e-3)
+    plain = n_total * K / (plain_ms * 1e-3)
+    return {"metric": "particle-steps/s", "value": batched, "plain_scene_by_scene": plain,
+            "batched_over_plain": batched / plain, "ms_per_step": ms / K, "plain_ms_per_step": plain_ms / K,
+            "scenes": len(specs), "particles": n_total, "steps": K, "tiling": [lpp, depth],
+            "device_bytes": mem, "setup_s": setup_s, "dtype": "f32 (compensated positions)",
+            "timing": "CUDA events on the batch's stream (batched) and per scene on its stream, summed (plain)",
+            "config": "256 cutting scenes, n log-uniform [5k, 200k] (nx=4nz, ny=2nz), v U[1e-4, 5e-3] cm/us, "
+                      "depth U[2, 10] dx, rake U[-20, 10] deg, Johnson-Cook A, B, n x U[0.9, 1.1], seed 1"}
+
+
+def run_serve(args, tiling) -> dict:
+    """Poisson request stream into one resident batch (continuous batching)."""
+    from iwf_mfree_gpu_3d_b200 import serve
+    lo, hi = args.serve_steps
+    reqs = serve.poisson_requests(rate=args.serve_rate, duration=args.serve_seconds, seed=2, n_lo=10000,
+                                  n_hi=args.serve_nmax, steps_lo=lo, steps_hi=hi)
+    srv = serve.Server(hbm_budget=150 * 10**9, chunk_steps=args.serve_chunk, tiling=tiling)
+    out = srv.run(reqs, horizon=4 * args.serve_seconds)
+    srv.close()
+    offered = sum(r.spec.n * r.spec.steps for r in reqs) / args.serve_seconds
+    return {"metric": "p50/p99 solve latency (s)", "p50_s": out["p50_s"], "p99_s": out["p99_s"],
+            "particle_steps_per_s": out["particle_steps_per_s"], "offered_particle_steps_per_s": offered,
+            "requests": out["offered"], "completed": out["completed"], "unfinished": out["unfinished"],
+            "elapsed_s": out["elapsed_s"], "chunk_steps": args.serve_chunk, "budget_bytes": 150 * 10**9,
+            "timing": "wall clock on the host, arrival to result read-back",
+            "config": f"Poisson {args.serve_rate}/s for {args.serve_seconds} s (seed 2), n log-uniform "
+                      f"[10k, {args.serve_nmax}], steps U[{lo}, {hi}]: the serving configuration "
+                      "(20/s, 600 s, [10k, 500k], U[500, 5000]) scaled down to finish in seconds"}
 
 
 def run_e2e(sc, args, opts, dist, local_rank) -> dict:

@@ -324,6 +324,11 @@ int mfree_batch_get_tiling(mfree_batch *b, int *lanes_per_particle, int *tile_de
  * (the smoothing length), which the bit-exact cell ids and order require.
  * *ms_best: time per step of the chosen tiling (may be NULL). */
 int mfree_batch_autotune(mfree_batch *b, int trial_steps, int *lanes_per_particle, int *tile_depth, double *ms_best);
+/* waits for the batch's queued work; CUDA-event timer on the batch's stream
+ * (device milliseconds between start and stop) */
+int mfree_batch_sync(mfree_batch *b);
+int mfree_batch_timer_start(mfree_batch *b);
+int mfree_batch_timer_stop(mfree_batch *b, double *ms);
 /* device bytes a context holds (state, scratch and tools) */
 int mfree_device_bytes(const mfree_ctx *ctx, size_t *bytes);
 /* device bytes mfree_create + mfree_set_grid will take for n particles and

@@ -41,7 +41,8 @@ EXPORTS = [
     "mfree_probe_fp32_peak", "mfree_timer_start", "mfree_timer_stop", "mfree_set_device",
     "mfree_cell_list_static", "mfree_batch_create", "mfree_batch_destroy", "mfree_batch_admit", "mfree_batch_step",
     "mfree_batch_query", "mfree_batch_context", "mfree_batch_retire", "mfree_batch_info", "mfree_batch_set_tiling",
-    "mfree_batch_get_tiling", "mfree_batch_autotune", "mfree_device_bytes", "mfree_scene_bytes",
+    "mfree_batch_get_tiling", "mfree_batch_autotune", "mfree_batch_sync", "mfree_batch_timer_start",
+    "mfree_batch_timer_stop", "mfree_device_bytes", "mfree_scene_bytes",
 ]
 ERR_BUDGET = -7
 KERNELS = ["clock", "hash", "scan_reduce", "scan_top", "scan_down", "scatter", "cell_fixup", "gather_predict",
@@ -149,6 +150,9 @@ def lib(path: str = LIB_PATH):
     L.mfree_batch_set_tiling.argtypes = [P, I, I]
     L.mfree_batch_get_tiling.argtypes = [P, ip, ip]
     L.mfree_batch_autotune.argtypes = [P, I, ip, ip, C.POINTER(C.c_double)]
+    L.mfree_batch_sync.argtypes = [P]
+    L.mfree_batch_timer_start.argtypes = [P]
+    L.mfree_batch_timer_stop.argtypes = [P, C.POINTER(C.c_double)]
     L.mfree_device_bytes.argtypes = [P, C.POINTER(S)]
     L.mfree_scene_bytes.argtypes = [I, LL]
     L.mfree_scene_bytes.restype = S
@@ -516,6 +520,18 @@ class Batch:
         a, b, ms = C.c_int(), C.c_int(), C.c_double()
         _check(self.L.mfree_batch_autotune(self.h, int(trial_steps), C.byref(a), C.byref(b), C.byref(ms)))
         return a.value, b.value, ms.value
+
+    def sync(self):
+        _check(self.L.mfree_batch_sync(self.h))
+
+    def timer_start(self):
+        _check(self.L.mfree_batch_timer_start(self.h))
+
+    def timer_stop(self) -> float:
+        """Device milliseconds since timer_start (CUDA events on the batch's stream)."""
+        ms = C.c_double()
+        _check(self.L.mfree_batch_timer_stop(self.h, C.byref(ms)))
+        return ms.value
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:

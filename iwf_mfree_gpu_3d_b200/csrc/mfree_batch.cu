@@ -59,6 +59,7 @@ struct mfree_batch {
     bool dirty = true;
     int table_record_every = -1;
     cudaGraphExec_t graph = nullptr;
+    cudaEvent_t timer[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -239,6 +240,8 @@ int mfree_batch_destroy(mfree_batch *b) {
             mfree_destroy(sl.c);
         }
     if (b->d_table) cudaFree(b->d_table);
+    for (auto e : b->timer)
+        if (e) cudaEventDestroy(e);
     if (b->own_stream) cudaStreamDestroy(b->stream);
     delete b;
     return MFREE_OK;
@@ -449,6 +452,30 @@ int mfree_batch_autotune(mfree_batch *b, int trial_steps, int *lpp_out, int *tz_
     if (lpp_out) *lpp_out = blpp;
     if (tz_out) *tz_out = btz;
     if (ms_best) *ms_best = best / trial_steps;
+    return MFREE_OK;
+}
+
+int mfree_batch_sync(mfree_batch *b) {
+    if (!b) return fail(MFREE_ERR_ARG, "mfree_batch_sync: null batch");
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    return MFREE_OK;
+}
+
+int mfree_batch_timer_start(mfree_batch *b) {
+    if (!b) return fail(MFREE_ERR_ARG, "mfree_batch_timer_start: null batch");
+    for (auto &e : b->timer)
+        if (!e) CUDA_TRY(cudaEventCreate(&e));
+    CUDA_TRY(cudaEventRecord(b->timer[0], b->stream));
+    return MFREE_OK;
+}
+
+int mfree_batch_timer_stop(mfree_batch *b, double *ms) {
+    if (!b || !ms || !b->timer[0]) return fail(MFREE_ERR_ARG, "mfree_batch_timer_stop: no timer started");
+    CUDA_TRY(cudaEventRecord(b->timer[1], b->stream));
+    CUDA_TRY(cudaEventSynchronize(b->timer[1]));
+    float f = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&f, b->timer[0], b->timer[1]));
+    *ms = f;
     return MFREE_OK;
 }
 
