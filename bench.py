@@ -70,7 +70,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["1m", "8k"], default="1m")
+    ap.add_argument("--workload", choices=["1m", "8k", "grain"], default="1m")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lpp", type=int, default=0, help="lanes per particle (0 = default)")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving measurements")
@@ -88,18 +88,25 @@ def make_scene(workload: str, seed: int = 0, precision: int = 0):
     from iwf_mfree_gpu_3d_b200 import scenes
     if workload == "8k":
         return scenes.small_scene(seed=seed, precision=precision)
+    if workload == "grain":
+        return scenes.single_grain(seed=seed)  # compensated positions, as the configuration asks
     return scenes.million_scene(seed=seed, precision=precision)
 
 
 def workload_config(workload: str, sc) -> dict:
-    return {"workload": ("orthogonal cutting 200x100x50 steel block (1,000,000 particles), CSPM + artificial "
-                         "stress + PSE, Johnson-Cook, wedge contact" if workload == "1m" else
-                         "orthogonal cutting 40x20x10 steel block (8,000 particles), Brookshaw, artificial "
-                         "stress, Johnson-Cook, wedge contact"),
+    names = {"1m": "orthogonal cutting 200x100x50 steel block (1,000,000 particles), CSPM + artificial "
+                   "stress + PSE, Johnson-Cook, wedge contact",
+             "8k": "orthogonal cutting 40x20x10 steel block (8,000 particles), Brookshaw, artificial "
+                   "stress, Johnson-Cook, wedge contact",
+             "grain": "single-grain cutting, 400x160x64 steel block (4,096,000 particles) + the grain volume "
+                      "as diamond tool particles, 1,280-triangle truncated icosphere (radius 20 dx, -10 deg rake) "
+                      "at 30 m/s, depth 8 dx, Brookshaw, compensated positions"}
+    return {"workload": names[workload],
             "particles": sc.n, "dx_cm": 1e-3, "h_over_dx": 1.3, "dt_us": sc.dt,
             "cspm": bool(sc.options["cspm"]), "conduction": ["none", "brookshaw", "pse"][sc.options["conduction"]],
-            "l2": "inputs larger than L2 (particle state ~0.5 GB)" if workload == "1m" else
-                  "inputs smaller than L2 (8k particles)",
+            "l2": {"1m": "inputs larger than L2 (particle state ~0.5 GB)",
+                   "grain": "inputs larger than L2 (particle state ~2.9 GB)"}.get(
+                       workload, "inputs smaller than L2 (8k particles)"),
             "parallelism": "one independent scene per GPU"}
 
 
@@ -198,6 +205,23 @@ def read_traffic() -> float | None:
             except ValueError:
                 return None
     return None
+
+
+def hbm_roofline(rate: float, sc) -> dict:
+    """Whole-step HBM roofline: the compulsory particle state crossing HBM once
+    per step (152 B read + 144 B written + 8 B sort key; the precision form adds
+    24 + 24 B of low parts) times the rate, against the measured copy bandwidth."""
+    b_alg = 352 if sc.options.get("precision") else 304
+    peak, src = 6650.0, "fallback 6.65 TB/s (no MEASURED_PEAKS.json)"
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, src = float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, KeyError, ValueError):
+        pass
+    gbs = rate * b_alg / 1e9
+    return {"algorithmic_bytes_per_particle_step": b_alg, "achieved_gbs": gbs, "peak_gbs": peak,
+            "frac": gbs / peak, "peak_source": src,
+            "note": "the step is bound by the pair kernel's FP32 pipe, not by HBM"}
 
 
 # -------------------------------------------------------------- oracle ----
@@ -325,7 +349,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     ik_ms, ik_n = ktimes["interact"]
     ik_avg = ik_ms / max(ik_n, 1)
     achieved = flops_launch / (ik_avg * 1e-3) / 1e12
-    traffic = read_traffic()
+    traffic = read_traffic() if args.workload == "1m" else None  # the ncu capture is of the 1M scene
     roofline = {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
                 "frac": achieved / peak_fp32,
                 "traffic": traffic,
@@ -338,14 +362,16 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded jittered lattice, generated wedge tool)",
+            "data": "synthetic (seeded jittered lattice, generated " +
+                    ("truncated-icosphere grain)" if args.workload == "grain" else "wedge tool)"),
             "config": workload_config(args.workload, sc),
             "roofline": roofline,
             "e2e": e2e,
             "gpu_launches": int(sum(v[1] for v in ktimes.values())),
             "kernel_ms_per_step": step_ms_dev,
             "clocks": clk.summary(),
-            "counters": counters}
+            "counters": counters,
+            "hbm": hbm_roofline(value, sc)}
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.workload)
     if world == 1 and not args.no_extras:

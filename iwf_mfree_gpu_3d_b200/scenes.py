@@ -283,13 +283,43 @@ def truncated_grain(radius: float, rake_deg: float = -10.0, cut: float = 0.5):
     return v, f
 
 
+def inside_mesh(points: np.ndarray, verts: np.ndarray, tris: np.ndarray, chunk: int = 2048) -> np.ndarray:
+    """Points inside a closed triangle mesh: parity of the hits of a +z ray
+    (Moller-Trumbore, the test the reference's contact uses)."""
+    V = verts.astype(np.float64)
+    v0, v1, v2 = V[tris[:, 0]], V[tris[:, 1]], V[tris[:, 2]]
+    e1, e2 = v1 - v0, v2 - v0
+    hv = np.stack([-e2[:, 1], e2[:, 0], np.zeros(len(e2))], 1)  # cross((0, 0, 1), e2)
+    a = np.einsum("ij,ij->i", e1, hv)
+    ok = np.abs(a) > 1e-12
+    f = np.where(ok, 1.0 / np.where(ok, a, 1.0), 0.0)
+    out = np.zeros(len(points), bool)
+    P = points.astype(np.float64)
+    for k in range(0, len(P), chunk):
+        sv = P[k:k + chunk, None, :] - v0[None]
+        u = f * np.einsum("mtj,tj->mt", sv, hv)
+        q = np.cross(sv, e1[None])
+        v = f * q[..., 2]
+        t = f * np.einsum("tj,mtj->mt", e2, q)
+        hit = ok & (u >= 0) & (u <= 1) & (v >= 0) & (u + v <= 1) & (t > 1e-12)
+        out[k:k + chunk] = (hit.sum(1) % 2) == 1
+    return out
+
+
 def single_grain(nx: int = 400, ny: int = 160, nz: int = 64, dx: float = 1.0e-3, v_tool: float = 3.0e-3,
-                 depth: float = 8.0, seed: int = 0, precision: int = 1, engage: float = 0.05) -> Scene:
+                 depth: float = 8.0, seed: int = 0, precision: int = 1, engage: float = 0.05,
+                 tool_particles: bool = True, radius: float = 20.0) -> Scene:
     """Single-grain cutting: a 1,280-triangle truncated icosphere of radius
-    20*dx at 30 m/s, depth of cut 8*dx, Brookshaw conduction."""
+    radius*dx (20 by default) at 30 m/s, depth of cut 8*dx, Brookshaw
+    conduction, compensated positions.  With
+    tool_particles, the grain's volume outside the workpiece is sampled on the
+    lattice spacing into tool particles (tool_p = 1) with diamond constants
+    (k = 2200 W/mK, cp = 520 J/kgK, rho = 3500 kg/m^3, as the reference's
+    single-grain setups, benchmarks_single_grain.cu:176,185-188), so heat flows
+    into the tool through the particles the way the reference does it."""
     sc = orthogonal_cutting(nx, ny, nz, dx=dx, v_tool=v_tool, depth=depth, seed=seed,
                             precision=precision, name=f"grain_{nx}x{ny}x{nz}")
-    R = 20.0 * dx
+    R = radius * dx
     v, f = truncated_grain(R)
     lx = (nx - 1) * dx
     # place the flattened face on the +x face, its lowest point depth*dx below the top
@@ -297,6 +327,21 @@ def single_grain(nx: int = 400, ny: int = 160, nz: int = 64, dx: float = 1.0e-3,
     v[:, 0] += lx - engage * dx - v[:, 0].min()
     v[:, 2] += -depth * dx - v[:, 2].min()
     sc.tools = [Tool(verts=v.astype(np.float32), tris=f, vel=np.array([-v_tool, 0, 0], np.float32))]
+    if tool_particles:
+        lo, hi = v.min(0), v.max(0)
+        axes = [np.arange(lo[d] + 0.5 * dx, hi[d], dx) for d in range(3)]
+        g = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 3)
+        g = g[(g[:, 0] > lx + 0.5 * dx) & inside_mesh(g, v, f)]
+        m = len(g)
+        rho_d, cp_d, k_d = 3.5, 5.2e-6, 2.2e-10
+        sc.pos = np.concatenate([sc.pos, np.concatenate([g, np.zeros((m, 1))], 1).astype(np.float32)])
+        sc.vel = np.concatenate([sc.vel, np.zeros((m, 4), np.float32)])
+        sc.rho = np.concatenate([sc.rho, np.full(m, rho_d, np.float32)])
+        sc.T = np.concatenate([sc.T, np.full(m, sc.trml_wp["T_init"], np.float32)])
+        sc.h = np.concatenate([sc.h, np.full(m, sc.h[0], np.float32)])
+        sc.fixed = np.concatenate([sc.fixed, np.zeros(m, np.float32)])
+        sc.tool_p = np.concatenate([sc.tool_p, np.ones(m, np.float32)])
+        sc.trml_tool = dict(cp=cp_d, tq=0.0, k=k_d, alpha=k_d / (rho_d * cp_d), T_init=sc.trml_wp["T_init"], eta=0.0)
     pad = 15.0 * dx
     lo = np.minimum(sc.pos[:, :3].min(0), v.min(0)) - pad
     hi = np.maximum(sc.pos[:, :3].max(0), v.max(0)) + pad

@@ -89,6 +89,25 @@ def test_tool_particles_conduct_heat():
     sim.close()
 
 
+def test_single_grain_with_tool_particles_against_oracle():
+    """The single-grain configuration at small size: a truncated-icosphere
+    grain (1,280 triangles, radius 6 dx) cutting a 40 x 20 x 12 block, its
+    volume sampled into diamond tool particles (thermal contact the reference
+    way), compensated positions: relative L2 after 40 steps against the FP64
+    oracle, and heat reaching the tool particles."""
+    sc = scenes.single_grain(40, 20, 12, radius=6.0, depth=4.0, v_tool=3.0e-3)
+    tool = sc.tool_p == 1.0
+    assert tool.sum() > 300
+    sim, orc = _run(sc, 40)
+    g, o = gpu_state(sim), oracle_state(orc)
+    err = compare(g, o, sc)
+    print("single grain 40-step relative L2:", err)
+    assert err["blank_mismatch"] == 0
+    for k, v in dict(POS=5e-3, VEL=5e-3, S=5e-3, EPS_PL=2e-2, T=2e-2, RHO=5e-3).items():
+        assert err[k] < v, (k, err)
+    sim.close()
+
+
 def test_nan_rate_spreads_and_is_blanked():
     """A NaN rate is not blanked by itself (do_blanking only refuses to
     unblank, actions_gpu.cu:506-529): it spreads through the pair loop, the
