@@ -436,35 +436,27 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
         if (sl == 0) cp[25] = carry;
     }
     __syncwarp();
-    // ---- candidates: lane sl of the group scans the contiguous chunk
-    // [kb, ke) of the flattened stencil (columns in order); the column it is
-    // in and the record index advance in registers
+    // ---- candidates: lane sl takes candidates sl, sl + LPP, ... of the
+    // flattened stencil (consecutive lanes read consecutive records); the
+    // column it is in is kept in registers and reloaded only on a crossing
     const int total = cp[25];
-    const int per = (total + LPP - 1) / LPP;
-    int maxper = per;
+    int maxtotal = total;
 #pragma unroll
-    for (int o = 16; o >= LPP; o >>= 1) maxper = max(maxper, __shfl_xor_sync(0xffffffffu, maxper, o));
-    const int kb = min(sl * per, total), ke = min(kb + per, total);
-    // visits the candidates of the chunk, one per step of the group, and
-    // calls fn(j, active) on every step (active false past the chunk's end)
+    for (int o = 16; o >= LPP; o >>= 1) maxtotal = max(maxtotal, __shfl_xor_sync(0xffffffffu, maxtotal, o));
     auto scan = [&](auto &&fn) {
-        int col = 0;
-        while (col < 24 && cp[col + 1] <= kb) col++;
-        int cend = cp[col + 1];
-        int j = cb[col] + (kb - cp[col]);
+        int col = 0, cend = cp[1], base = cb[0];  // base = cb[col] - cp[col]
 #pragma unroll 2
-        for (int it = 0; it < maxper; it++) {
-            const int k = kb + it;
-            const bool act = k < ke;
+        for (int k0 = 0; k0 < maxtotal; k0 += LPP) {
+            const int k = k0 + sl;
+            const bool act = k < total;
             if (act) {
-                while (k >= cend) {  // next non-empty column (k < total keeps col <= 24)
+                while (k >= cend) {  // k < total keeps col <= 24
                     col++;
                     cend = cp[col + 1];
-                    j = cb[col];
+                    base = cb[col] - cp[col];
                 }
             }
-            fn(j, act);
-            j++;
+            fn(base + k, act);
         }
     };
     // ---- pass A: support test, PSE, queue
