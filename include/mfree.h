@@ -335,6 +335,27 @@ int mfree_device_bytes(const mfree_ctx *ctx, size_t *bytes);
  * num_cell grid cells, before tools: to check a budget before creating */
 size_t mfree_scene_bytes(int n, long long num_cell);
 
+/* ---- output in the reference's formats ------------------------------------
+ * Particles as legacy VTK, the reference's vtk_writer_write(particle_gpu*)
+ * (vtk_writer.cpp:78-262): the unblanked particles in sorted order with density,
+ * contact, Temperature, Fixed, Tool, EquivAccumPlasticStrain and Svm.  The state
+ * is snapshot on the context's stream by device copies; the copy to the host
+ * (on a stream of its own) and the file writing (on a host thread) overlap the
+ * steps that follow.  One particle output per context is in flight: the next
+ * call, mfree_output_wait and mfree_destroy wait for it; a failure of the
+ * writing is returned by the next of those calls. */
+int mfree_write_vtk(mfree_ctx *ctx, const char *path);
+int mfree_output_wait(mfree_ctx *ctx);
+/* tool meshes at the last step's time, one file for all tools with "id" and
+ * "active" point data (vtk_writer_write_unified, vtk_writer.cpp:307-386) */
+int mfree_write_vtk_tools(mfree_ctx *ctx, const char *path);
+/* the blanking box at the last step's time (vtk_writer_write_blanking, vtk_writer.cpp:22-77) */
+int mfree_write_vtk_blanking(mfree_ctx *ctx, const char *path);
+/* appends one line of the tool-force log, "%.9g %.9g %.9g " per tool and a
+ * newline (tool_forces::report, tool_3d_gpu.cu:53-69); the forces are those of
+ * the last recorded step, summed in a fixed order */
+int mfree_append_force_log(mfree_ctx *ctx, const char *path);
+
 /* ---- scene files (the reference's setup readers) ------------------------- */
 /* json_read_triangles (json_reader.cpp:108-117): MeshLab JSON */
 int mfree_read_mesh_json(const char *path, float **verts, int *nv, int **tris, int *nt);

@@ -42,7 +42,8 @@ EXPORTS = [
     "mfree_cell_list_static", "mfree_batch_create", "mfree_batch_destroy", "mfree_batch_admit", "mfree_batch_step",
     "mfree_batch_query", "mfree_batch_context", "mfree_batch_retire", "mfree_batch_info", "mfree_batch_set_tiling",
     "mfree_batch_get_tiling", "mfree_batch_autotune", "mfree_batch_sync", "mfree_batch_timer_start",
-    "mfree_batch_timer_stop", "mfree_device_bytes", "mfree_scene_bytes",
+    "mfree_batch_timer_stop", "mfree_device_bytes", "mfree_scene_bytes", "mfree_write_vtk", "mfree_output_wait",
+    "mfree_write_vtk_tools", "mfree_write_vtk_blanking", "mfree_append_force_log",
 ]
 ERR_BUDGET = -7
 KERNELS = ["clock", "hash", "scan_reduce", "scan_top", "scan_down", "scatter", "cell_fixup", "gather_predict",
@@ -156,6 +157,9 @@ def lib(path: str = LIB_PATH):
     L.mfree_device_bytes.argtypes = [P, C.POINTER(S)]
     L.mfree_scene_bytes.argtypes = [I, LL]
     L.mfree_scene_bytes.restype = S
+    for name in ("mfree_write_vtk", "mfree_write_vtk_tools", "mfree_write_vtk_blanking", "mfree_append_force_log"):
+        getattr(L, name).argtypes = [P, C.c_char_p]
+    L.mfree_output_wait.argtypes = [P]
     _lib = L
     return L
 
@@ -404,6 +408,23 @@ class Simulation:
         ip = C.POINTER(C.c_int)
         _check(self.L.mfree_get_cells(self.h, cs.ctypes.data_as(ip), ce.ctypes.data_as(ip)))
         return cs, ce
+
+    # -- output in the reference's formats (results/vtk_out_%06d.vtk etc.)
+    def write_vtk(self, path: str):
+        """Particles as legacy VTK; written in the background (output_wait joins)."""
+        _check(self.L.mfree_write_vtk(self.h, os.fsencode(path)))
+
+    def output_wait(self):
+        _check(self.L.mfree_output_wait(self.h))
+
+    def write_vtk_tools(self, path: str):
+        _check(self.L.mfree_write_vtk_tools(self.h, os.fsencode(path)))
+
+    def write_vtk_blanking(self, path: str):
+        _check(self.L.mfree_write_vtk_blanking(self.h, os.fsencode(path)))
+
+    def append_force_log(self, path: str):
+        _check(self.L.mfree_append_force_log(self.h, os.fsencode(path)))
 
     def device_bytes(self) -> int:
         """Device memory the context holds (state, scratch, tools)."""

@@ -32,6 +32,7 @@ namespace host {
 
 struct DevTool {
     HostTool host;
+    std::vector<float> verts;  // input vertices (x, y, z), for output
     int algorithm = MFREE_CONTACT_HASHED;
     float vel[3] = {0, 0, 0};
     float alpha = 0.1f, mu = 0.f;
@@ -103,6 +104,8 @@ struct mfree_ctx {
     mfree_batch *owner = nullptr;
     cudaStream_t home_stream = nullptr;
     unsigned long long version = 0;
+    // asynchronous particle output (mfree_output.cu), created on first use
+    struct OutputJob *output = nullptr;
 };
 
 
@@ -122,6 +125,8 @@ void invalidate_graphs(mfree_ctx *c);
 int alloc_ctx(int n, cudaStream_t stream, std::unique_ptr<mfree_ctx> &out);
 // a copy of c (configuration, tools, current state and clock) on stream s
 int clone_ctx(const mfree_ctx *c, cudaStream_t s, std::unique_ptr<mfree_ctx> &out);
+// waits for and frees the context's output job (mfree_output.cu)
+int finish_output(mfree_ctx *c, bool release);
 size_t scene_bytes(int n, long long num_cell);
 inline size_t single_table_bytes() { return 2 * sizeof(mfree::StepArgs) + 9 * sizeof(int); }
 // device memory the context holds, in bytes

@@ -558,6 +558,7 @@ int mfree_create(int n, const float *pos4, const float *vel4, const float *rho, 
 int mfree_destroy(mfree_ctx *c) {
     if (!c) return MFREE_OK;
     if (c->owner) return fail(MFREE_ERR_ARG, "mfree_destroy: the context belongs to a batch (retire it first)");
+    finish_output(c, true);
     cudaStreamSynchronize(c->stream);
     invalidate_graphs(c);
     for (auto &t : c->tools) {
@@ -695,6 +696,7 @@ int mfree_add_tool(mfree_ctx *c, const float *verts, int nv, const int *tris, in
     std::string err;
     if (!build_host_tool(t->host, verts, nv, tris, nt, err)) return fail(MFREE_ERR_ARG, "mfree_add_tool: " + err);
     t->algorithm = algorithm;
+    t->verts.assign(verts, verts + 3 * size_t(nv));
     for (int d = 0; d < 3; d++) t->vel[d] = vel[d];
     t->alpha = contact_alpha;
     t->mu = mu;
