@@ -63,7 +63,8 @@ struct IData {
 // gradient factor of cubic_spline (kernels.cuh:26-69): value w and
 // dfac = der*fac with grad W = dfac * (x_i - x_j)
 __device__ __forceinline__ void spline(float r2, float h1, float fac, float &w, float &dfac) {
-    const float rinv = rsqrtf(r2);
+    float rinv;  // r2 >= 1e-8 here: never a denormal
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rinv) : "f"(r2));
     const float r = r2 * rinv;
     const float q = r * h1;
     float val, der;
@@ -473,7 +474,9 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
             ins = !(r2 >= four_h2) && (r2 > 9.99999994e-9f);  // in_support()
             if (COND == MFREE_COND_PSE) {
                 const float4 Cj = rC[j];
-                pse = fmaf((Cj.z - I.T) * Cj.w, exp2f(pse_k * r2), pse);
+                float e2;
+                asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e2) : "f"(pse_k * r2));
+                pse = fmaf((Cj.z - I.T) * Cj.w, e2, pse);
             }
         }
         cnt += ins ? 1 : 0;
