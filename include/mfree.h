@@ -335,6 +335,16 @@ int mfree_device_bytes(const mfree_ctx *ctx, size_t *bytes);
  * num_cell grid cells, before tools: to check a budget before creating */
 size_t mfree_scene_bytes(int n, long long num_cell);
 
+/* ---- checkpoint and resume (no counterpart in the reference) ---------------
+ * mfree_export_state writes the context's configuration, tools (as their input
+ * meshes), device clock, last recorded tool forces and particle state into one
+ * binary record; with buf NULL it only sets *size to the bytes needed.
+ * mfree_import_state creates a context from such a record (stream NULL: a
+ * stream of its own); stepping it continues bitwise as the exported context
+ * would. */
+int mfree_export_state(mfree_ctx *ctx, void *buf, size_t *size);
+int mfree_import_state(const void *buf, size_t size, void *stream, mfree_ctx **out);
+
 /* ---- output in the reference's formats ------------------------------------
  * Particles as legacy VTK, the reference's vtk_writer_write(particle_gpu*)
  * (vtk_writer.cpp:78-262): the unblanked particles in sorted order with density,

@@ -43,7 +43,8 @@ EXPORTS = [
     "mfree_batch_query", "mfree_batch_context", "mfree_batch_retire", "mfree_batch_info", "mfree_batch_set_tiling",
     "mfree_batch_get_tiling", "mfree_batch_autotune", "mfree_batch_sync", "mfree_batch_timer_start",
     "mfree_batch_timer_stop", "mfree_device_bytes", "mfree_scene_bytes", "mfree_write_vtk", "mfree_output_wait",
-    "mfree_write_vtk_tools", "mfree_write_vtk_blanking", "mfree_append_force_log",
+    "mfree_write_vtk_tools", "mfree_write_vtk_blanking", "mfree_append_force_log", "mfree_export_state",
+    "mfree_import_state",
 ]
 ERR_BUDGET = -7
 KERNELS = ["clock", "hash", "scan_reduce", "scan_top", "scan_down", "scatter", "cell_fixup", "gather_predict",
@@ -160,6 +161,8 @@ def lib(path: str = LIB_PATH):
     for name in ("mfree_write_vtk", "mfree_write_vtk_tools", "mfree_write_vtk_blanking", "mfree_append_force_log"):
         getattr(L, name).argtypes = [P, C.c_char_p]
     L.mfree_output_wait.argtypes = [P]
+    L.mfree_export_state.argtypes = [P, P, C.POINTER(S)]
+    L.mfree_import_state.argtypes = [P, S, P, C.POINTER(P)]
     _lib = L
     return L
 
@@ -408,6 +411,29 @@ class Simulation:
         ip = C.POINTER(C.c_int)
         _check(self.L.mfree_get_cells(self.h, cs.ctypes.data_as(ip), ce.ctypes.data_as(ip)))
         return cs, ce
+
+    # -- checkpoint and resume
+    def export_state(self) -> bytes:
+        """The context (configuration, tools, clock, particle state) as one binary record."""
+        n = C.c_size_t()
+        _check(self.L.mfree_export_state(self.h, None, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        _check(self.L.mfree_export_state(self.h, buf, C.byref(n)))
+        return buf.raw[: n.value]
+
+    @classmethod
+    def import_state(cls, record: bytes, stream: Optional[int] = None) -> "Simulation":
+        """A new context from a record of export_state; it steps on exactly as the exported one."""
+        import struct
+        L = lib()
+        h = C.c_void_p()
+        buf = C.create_string_buffer(record, len(record))
+        _check(L.mfree_import_state(buf, len(record), C.c_void_p(stream) if stream else None, C.byref(h)))
+        sim = cls.__new__(cls)
+        sim.L = L
+        sim.h = h
+        sim.n_init, sim.num_tools = struct.unpack_from("<II", record, 12)
+        return sim
 
     # -- output in the reference's formats (results/vtk_out_%06d.vtk etc.)
     def write_vtk(self, path: str):

@@ -23,7 +23,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["mfree_sort.cu", "mfree_interact.cu", "mfree_contact.cu", "mfree_host.cu", "mfree_batch.cu",
-              "mfree_output.cu", "mfree_probe.cu", "mfree_static.cu"]
+              "mfree_output.cu", "mfree_state.cu", "mfree_probe.cu", "mfree_static.cu"]
 CPP_SOURCES = ["mfree_tool.cpp", "mfree_io.cpp"]
 
 

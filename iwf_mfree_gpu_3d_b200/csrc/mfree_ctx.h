@@ -121,6 +121,8 @@ int ready(mfree_ctx *c);
 int check_empty(mfree_ctx *c, bool wait);
 int note_active_count(mfree_ctx *c);
 void invalidate_graphs(mfree_ctx *c);
+// allocates the grid-sized scratch (cell counters, cell table, scan sums)
+int ensure_scratch(mfree_ctx *c);
 // allocates a context's device memory and stream (no state upload)
 int alloc_ctx(int n, cudaStream_t stream, std::unique_ptr<mfree_ctx> &out);
 // a copy of c (configuration, tools, current state and clock) on stream s

@@ -6,7 +6,8 @@ src/mfree_gpu_3d.cpp:75-218); this module has no counterpart there.  Requests
 ``api.Batch`` on the GPU and, between chunks of steps:
 
   * admits waiting requests in arrival order while their device memory fits
-    the budget (continuous batching: a request joins while others run);
+    the budget (continuous batching: a request joins while others run); a
+    request that would not fit even an empty batch is rejected;
   * enqueues a chunk of steps of every running scene (the call returns once
     the work is queued, so the host builds the next scenes while the GPU
     computes);
@@ -115,6 +116,7 @@ class Server:
         waiting: collections.deque = collections.deque()
         active: Dict[int, tuple] = {}
         results: List[Result] = []
+        rejected: List[Request] = []
         t0 = clock()
         psteps = 0
         chunks = 0
@@ -129,11 +131,17 @@ class Server:
                 req = waiting[0]
                 scene = scenes.mixed_scene(req.spec, precision=self.precision)
                 if not self._fits(scene):
+                    if self.batch.info()["scenes"] == 0:  # larger than the whole budget
+                        rejected.append(waiting.popleft())
+                        continue
                     break
                 sim = api.Simulation.from_scene(scene)
                 slot = self.batch.admit(sim, req.spec.steps)
                 if slot is None:
                     sim.close()
+                    if self.batch.info()["scenes"] == 0:
+                        rejected.append(waiting.popleft())
+                        continue
                     break
                 waiting.popleft()
                 active[slot] = (req, clock() - t0, sim)
@@ -165,6 +173,7 @@ class Server:
             results=results,
             completed=len(results),
             offered=len(requests),
+            rejected=len(rejected),
             unfinished=len(active) + len(waiting) + len(pending),
             elapsed_s=elapsed,
             particle_steps=psteps,

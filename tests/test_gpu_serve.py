@@ -87,3 +87,12 @@ def test_admission_waits_for_the_memory_budget():
     res = sorted(out["results"], key=lambda r: r.admitted)
     for a, b in zip(res, res[1:]):
         assert b.admitted >= a.finished  # one at a time
+
+
+def test_request_larger_than_the_budget_is_rejected():
+    reqs = _requests(2, seed=3, steps=(10, 20), n=(2600, 2900), spacing=0.0)
+    one = api.scene_bytes(reqs[0].spec.n, serve.grid_cells(scenes.mixed_scene(reqs[0].spec)))
+    srv = serve.Server(hbm_budget=one // 2, chunk_steps=5, tool_bytes=0)
+    out = srv.run(reqs, clock=_ticks())
+    srv.close()
+    assert out["completed"] == 0 and out["rejected"] == 2 and out["unfinished"] == 0
