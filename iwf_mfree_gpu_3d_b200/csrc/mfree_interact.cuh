@@ -298,13 +298,15 @@ constexpr int HX = TX + 4, HY = TY + 4;
 constexpr int CSROW = TILE_Z_MAX + 5;  // cell starts kept per halo column
 constexpr int NHC = HX * HY;           // halo columns
 constexpr int NTC = TX * TY;           // target columns
-constexpr int TILE_THREADS = 512;
-constexpr int TILE_WARPS = TILE_THREADS / 32;
+// threads per block: with CSPM, 640 (96 registers a thread, some spilled) beat
+// 512 (128 registers) by about 2 % on the 1M-particle scene; without CSPM, 512
+// were faster by about as much
+template <bool CSPM> __host__ __device__ constexpr int tile_threads() { return CSPM ? 640 : 512; }
 constexpr int TCAP = 320;              // targets per pass of a tile
 constexpr int QCAP_T = 96;             // in-support queue per target before the rescan path
 constexpr int SMEM_LIMIT = 232448;     // per-block shared memory of sm_100
 
-template <int LPP> struct TileSmem {
+template <int LPP, int TILE_WARPS> struct TileSmem {
     static constexpr int G = 32 / LPP;
     float res[TCAP][NRES + 1];
     int tgt[TCAP];       // sorted index of each target of the pass
@@ -322,12 +324,14 @@ template <int LPP> struct TileSmem {
 };
 __host__ __device__ constexpr size_t round128(size_t b) { return (b + 127) / 128 * 128; }
 // shared memory: the tables, the scene's arguments, the staged records
-template <int LPP> __host__ __device__ constexpr size_t args_offset() { return round128(sizeof(TileSmem<LPP>)); }
-template <int LPP> __host__ __device__ constexpr size_t rec_offset() {
-    return args_offset<LPP>() + round128(sizeof(StepArgs));
+template <int LPP, int W> __host__ __device__ constexpr size_t args_offset() {
+    return round128(sizeof(TileSmem<LPP, W>));
 }
-template <int LPP> __host__ __device__ constexpr int rec_capacity() {
-    return int((SMEM_LIMIT - rec_offset<LPP>()) / (REC_N * sizeof(float4)));
+template <int LPP, int W> __host__ __device__ constexpr size_t rec_offset() {
+    return args_offset<LPP, W>() + round128(sizeof(StepArgs));
+}
+template <int LPP, int W> __host__ __device__ constexpr int rec_capacity() {
+    return int((SMEM_LIMIT - rec_offset<LPP, W>()) / (REC_N * sizeof(float4)));
 }
 __host__ __device__ inline int tile_count(const Params &P) {
     return ((P.gnx + TX - 1) / TX) * ((P.gny + TY - 1) / TY) * ((P.gnz + P.tile_z - 1) / P.tile_z);
@@ -570,7 +574,10 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
 // cell starts, staging, then the targets in passes of TCAP.  Returns false
 // when a staging wait ran out (the caller leaves the kernel).
 template <int LPP, bool CSPM, int COND, bool PREC, int CAP>
-__device__ __forceinline__ bool interact_tile(const StepArgs &a, TileSmem<LPP> &sm, float4 *sarr, int tile) {
+__device__ __forceinline__ bool interact_tile(const StepArgs &a, TileSmem<LPP, tile_threads<CSPM>() / 32> &sm,
+                                              float4 *sarr, int tile) {
+    constexpr int TILE_THREADS = tile_threads<CSPM>();
+    constexpr int TILE_WARPS = TILE_THREADS / 32;
     constexpr int G = 32 / LPP;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane / LPP, sl = lane - g * LPP;
@@ -733,7 +740,7 @@ __device__ __forceinline__ bool interact_tile(const StepArgs &a, TileSmem<LPP> &
     return true;
 }
 
-template <int LPP> __device__ __forceinline__ void init_tile_smem(TileSmem<LPP> &sm) {
+template <class SM> __device__ __forceinline__ void init_tile_smem(SM &sm) {
     if (threadIdx.x == 0) {
         mbar_init(&sm.bar, 1);
         sm.parity = 0;
@@ -746,13 +753,14 @@ template <int LPP> __device__ __forceinline__ void init_tile_smem(TileSmem<LPP> 
 // (one queue); a block copies a scene's arguments into shared memory when its
 // next tile belongs to another scene than its last one
 template <int LPP, bool CSPM, int COND, bool PREC>
-__global__ void __launch_bounds__(TILE_THREADS, 1) kb_interact(BatchTable T) {
-    constexpr int CAP = rec_capacity<LPP>();
+__global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTable T) {
+    constexpr int W = tile_threads<CSPM>() / 32;
+    constexpr int CAP = rec_capacity<LPP, W>();
     extern __shared__ __align__(128) unsigned char dyn[];
-    TileSmem<LPP> &sm = *reinterpret_cast<TileSmem<LPP> *>(dyn);
-    StepArgs &sa = *reinterpret_cast<StepArgs *>(dyn + args_offset<LPP>());
-    float4 *sarr = reinterpret_cast<float4 *>(dyn + rec_offset<LPP>());
-    init_tile_smem<LPP>(sm);
+    TileSmem<LPP, W> &sm = *reinterpret_cast<TileSmem<LPP, W> *>(dyn);
+    StepArgs &sa = *reinterpret_cast<StepArgs *>(dyn + args_offset<LPP, W>());
+    float4 *sarr = reinterpret_cast<float4 *>(dyn + rec_offset<LPP, W>());
+    init_tile_smem(sm);
     const int total = T.itile[T.nscenes];
     int cur = -1;
     for (;;) {
@@ -780,7 +788,7 @@ template <int LPP, bool CSPM, int COND, bool PREC> struct Variant {
         auto kern = kb_interact<LPP, CSPM, COND, PREC>;
         if (grid <= 0)  // prepare only: raise the shared-memory limit (outside any graph capture)
             return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT);
-        kern<<<grid, TILE_THREADS, SMEM_LIMIT, s>>>(T);
+        kern<<<grid, tile_threads<CSPM>(), SMEM_LIMIT, s>>>(T);
         return cudaGetLastError();
     }
 };
