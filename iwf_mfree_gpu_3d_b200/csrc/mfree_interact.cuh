@@ -34,23 +34,21 @@
 
 namespace mfree {
 
-// 2x2 minors of the column-major (GLM) 3x3 in m[c*3+r]
-__device__ __forceinline__ float det3(const float *m) {
-    auto A = [&](int r, int c) { return m[c * 3 + r]; };
-    return A(0, 0) * (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) - A(1, 0) * (A(0, 1) * A(2, 2) - A(0, 2) * A(2, 1)) +
-           A(2, 0) * (A(0, 1) * A(1, 2) - A(0, 2) * A(1, 1));
+// The CSPM matrix B = sum V_j (x_i - x_j) (x) grad W_ij is symmetric (grad W
+// is parallel to x_i - x_j), and so is its inverse: both are kept as the six
+// entries xx, yy, zz, xy, xz, yz.
+__device__ __forceinline__ float det3s(const float *m) {
+    return m[0] * (m[1] * m[2] - m[5] * m[5]) - m[3] * (m[3] * m[2] - m[4] * m[5]) + m[4] * (m[3] * m[5] - m[4] * m[1]);
 }
-__device__ __forceinline__ void inv3(const float *m, float det, float *o) {
-    auto A = [&](int r, int c) { return m[c * 3 + r]; };
+// inverse by cofactors (cofactor(r, c) / det; symmetric)
+__device__ __forceinline__ void inv3s(const float *m, float det, float *o) {
     const float id = 1.0f / det;
-#pragma unroll
-    for (int r = 0; r < 3; r++)
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            // o(r,c) = cofactor(c,r)/det
-            const int r0 = (c + 1) % 3, r1 = (c + 2) % 3, c0 = (r + 1) % 3, c1 = (r + 2) % 3;
-            o[c * 3 + r] = (A(r0, c0) * A(r1, c1) - A(r0, c1) * A(r1, c0)) * id;
-        }
+    o[0] = (m[1] * m[2] - m[5] * m[5]) * id;  // xx
+    o[1] = (m[0] * m[2] - m[4] * m[4]) * id;  // yy
+    o[2] = (m[0] * m[1] - m[3] * m[3]) * id;  // zz
+    o[3] = (m[4] * m[5] - m[3] * m[2]) * id;  // xy
+    o[4] = (m[3] * m[5] - m[4] * m[1]) * id;  // xz
+    o[5] = (m[3] * m[4] - m[0] * m[5]) * id;  // yz
 }
 
 struct IData {
@@ -90,9 +88,9 @@ __device__ __forceinline__ void pair_body(const Params &P, const IData &I, const
     spline(r2, I.h1, I.fac, w, dfac);
     float gx = dfac * dx, gy = dfac * dy, gz = dfac * dz;
     if (CSPM) {
-        const float ux = gx * invB[0] + gy * invB[3] + gz * invB[6];
-        const float uy = gx * invB[1] + gy * invB[4] + gz * invB[7];
-        const float uz = gx * invB[2] + gy * invB[5] + gz * invB[8];
+        const float ux = gx * invB[0] + gy * invB[3] + gz * invB[4];
+        const float uy = gx * invB[3] + gy * invB[1] + gz * invB[5];
+        const float uz = gx * invB[4] + gy * invB[5] + gz * invB[2];
         gx = ux; gy = uy; gz = uz;
     }
     const bool mech = !(I.tool == 1.f) && !(Pj.w == 1.f);
@@ -513,24 +511,25 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
         });
     };
     // ---- CSPM matrix over the in-support neighbours (interactions_gpu.cu:227-295)
-    float invB[9] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};
+    float invB[6] = {1.f, 1.f, 1.f, 0.f, 0.f, 0.f};
     if (CSPM) {
-        float Bm[9];
+        float Bm[6];  // xx, yy, zz, xy, xz, yz
 #pragma unroll
-        for (int k = 0; k < 9; k++) Bm[k] = 0.f;
+        for (int k = 0; k < 6; k++) Bm[k] = 0.f;
         auto bterm = [&](int j) {
             const float4 Pj = rP[j];
             if (I.tool == 1.f || Pj.w == 1.f) return;
             const float dx = I.x - Pj.x, dy = I.y - Pj.y, dz = I.z - Pj.z;
             float w, dfac;
             spline(dist2_rn(dx, dy, dz), I.h1, I.fac, w, dfac);
-            const float vol = -rC[j].w;
-            const float d[3] = {dx, dy, dz};
-            const float gr[3] = {dfac * dx, dfac * dy, dfac * dz};
-#pragma unroll
-            for (int c = 0; c < 3; c++)
-#pragma unroll
-                for (int r = 0; r < 3; r++) Bm[c * 3 + r] = fmaf(vol * d[r], gr[c], Bm[c * 3 + r]);
+            const float sv = -rC[j].w * dfac;  // -V_j dfac: B += sv d (x) d
+            const float tx = sv * dx, ty = sv * dy, tz = sv * dz;
+            Bm[0] = fmaf(tx, dx, Bm[0]);
+            Bm[1] = fmaf(ty, dy, Bm[1]);
+            Bm[2] = fmaf(tz, dz, Bm[2]);
+            Bm[3] = fmaf(tx, dy, Bm[3]);
+            Bm[4] = fmaf(tx, dz, Bm[4]);
+            Bm[5] = fmaf(ty, dz, Bm[5]);
         };
         for (int q0 = 0; q0 < maxq; q0 += LPP) {
             const int q = q0 + sl;
@@ -540,9 +539,9 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
 #pragma unroll
         for (int o = LPP / 2; o >= 1; o >>= 1)
 #pragma unroll
-            for (int k = 0; k < 9; k++) Bm[k] += __shfl_xor_sync(0xffffffffu, Bm[k], o);
-        const float det = det3(Bm);
-        if (det > 9.99999994e-9f) inv3(Bm, det, invB);
+            for (int k = 0; k < 6; k++) Bm[k] += __shfl_xor_sync(0xffffffffu, Bm[k], o);
+        const float det = det3s(Bm);
+        if (det > 9.99999994e-9f) inv3s(Bm, det, invB);
     }
     // ---- pair body over the in-support neighbours
     float acc[19];
