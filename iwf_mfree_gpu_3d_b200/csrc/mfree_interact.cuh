@@ -465,7 +465,7 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
     // ---- pass A: support test, PSE, queue
     const float pse_k = -1.44269504088896341f * I.h1 * I.h1;  // exp(-r^2/h^2) = 2^(pse_k r^2)
     const float four_h2 = __fmul_rn(__fmul_rn(4.0f, I.h), I.h);
-    int qn = 0, cnt = 0;
+    int qn = 0;  // in-support neighbours of the target (the group's ballots: the same in every lane)
     float pse = 0.f;
     scan([&](int j, bool act) {
         bool ins = false;
@@ -481,7 +481,6 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
                 pse = fmaf((Cj.z - I.T) * Cj.w, e2, pse);
             }
         }
-        cnt += ins ? 1 : 0;
         const unsigned m = __ballot_sync(0xffffffffu, ins) & gmask;
         if (ins) {
             const int pos = qn + __popc(m & lt_mask);
@@ -489,6 +488,11 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
         }
         qn += __popc(m);
     });
+    if (COND == MFREE_COND_PSE) {  // the PSE sum waits in the target's result slot
+#pragma unroll
+        for (int o = LPP / 2; o >= 1; o >>= 1) pse += __shfl_xor_sync(0xffffffffu, pse, o);
+        if (sl == 0 && valid) sm.res[tt][18] = pse;
+    }
     __syncwarp();
     const int qv = min(qn, QCAP_T);
     int maxq = qv;
@@ -553,18 +557,17 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
         if (q < qv) pterm(qq[q]);
     }
     if (overflow) for_overflow(pterm);
-    if (COND == MFREE_COND_PSE) acc[18] = pse;
+    constexpr int NACC = COND == MFREE_COND_PSE ? 18 : 19;  // (slot 18 holds the PSE sum already)
 #pragma unroll
     for (int o = LPP / 2; o >= 1; o >>= 1) {
 #pragma unroll
-        for (int k = 0; k < 19; k++) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
-        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        for (int k = 0; k < NACC; k++) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
     }
     if (sl == 0 && valid) {
         float *rs = sm.res[tt];
 #pragma unroll
-        for (int k = 0; k < 19; k++) rs[k] = acc[k];
-        rs[19] = __int_as_float(cnt);
+        for (int k = 0; k < NACC; k++) rs[k] = acc[k];
+        rs[19] = __int_as_float(qn);
     }
     __syncwarp();
 }
