@@ -296,10 +296,11 @@ constexpr int HX = TX + 4, HY = TY + 4;
 constexpr int CSROW = TILE_Z_MAX + 5;  // cell starts kept per halo column
 constexpr int NHC = HX * HY;           // halo columns
 constexpr int NTC = TX * TY;           // target columns
-// threads per block: with CSPM, 640 (96 registers a thread, some spilled) beat
-// 512 (128 registers) by about 2 % on the 1M-particle scene; without CSPM, 512
-// were faster by about as much
-template <bool CSPM> __host__ __device__ constexpr int tile_threads() { return CSPM ? 640 : 512; }
+// threads per block: 640 (20 warps, 96 registers a thread, a few spilled)
+// beat 512 (16 warps, 128 registers) by about 2 % on the 1M-particle scene
+// (CSPM + PSE) and by about 1 % on the mixed-size scenes (Brookshaw); 672 and
+// more threads leave at most 80 registers a thread, and the spills win
+template <bool CSPM> __host__ __device__ constexpr int tile_threads() { return 640; }
 constexpr int TCAP = 320;              // targets per pass of a tile
 constexpr int QCAP_T = 96;             // in-support queue per target before the rescan path
 constexpr int SMEM_LIMIT = 232448;     // per-block shared memory of sm_100
