@@ -144,7 +144,7 @@ int build_table(mfree_batch *b, int record_every) {
     return MFREE_OK;
 }
 
-// the kernels of one batch step (record_mode as k_clock; 2 = every
+// the kernels of one batch step (record_mode as kb_clock; 2 = every
 // Params::record_every steps of each scene's own step index)
 int enqueue_batch_step(mfree_batch *b, int record_mode) {
     const BatchTable &T = b->T;

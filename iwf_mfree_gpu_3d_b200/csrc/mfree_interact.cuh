@@ -12,22 +12,24 @@
 //   do_plasticity_johnson_cook actions_gpu.cu:371-449
 //   do_reset_contact_forces, do_boundary_conditions(_thermal), do_move_tool_particles
 //                             leap_frog.cu:102-119, actions_gpu.cu:55-68,451-487
-//                             (particles inside a tool box defer these to k_finalize)
+//                             (particles inside a tool box defer these to kb_finalize)
 //
-// Work decomposition: a persistent block (512 threads, one per SM) pulls
-// tiles of 4 x 4 x 6 cells from a work counter.  The tile's particles are 16
-// contiguous ranges of the sorted order; the records their 5x5x5 stencils
-// touch are the 64 contiguous column ranges of the 8 x 8 x 10-cell halo,
-// staged into shared memory with one bulk copy per column (TMA
+// Work decomposition: a persistent block (640 threads, one per SM) pulls
+// tiles of 4 x 4 x D cells (D = Params::tile_z, 6 by default) of every scene
+// of the table from one work counter.  The tile's particles are 16 contiguous
+// ranges of the sorted order; the records their 5x5x5 stencils touch are the
+// 64 contiguous column ranges of the 8 x 8 x (D+4)-cell halo, staged into
+// shared memory with one bulk copy per column and record array (TMA
 // cp.async.bulk, completion counted on an mbarrier, bounded waits).  Each
 // target is served by a group of LPP lanes.  Pass A streams the target's
 // candidates (25 column ranges of the staged halo) through the lanes: support
-// test, PSE (which sums every stencil candidate), CSPM matrix, and a ballot
-// that compacts the in-support neighbours into a queue.  Pass B runs the full
-// pair body on the queue only -- the reference evaluates every candidate,
-// ~3.5x more work, and candidates outside the support contribute exact zeros
-// there.  Accumulators are reduced across the group with xor shuffles; then
-// one thread per target runs the per-particle epilogue.
+// test, PSE (which sums every stencil candidate) and a ballot that compacts
+// the in-support neighbours into a queue.  The CSPM pass (symmetric matrix)
+// and the pair pass run on the queue only -- the reference evaluates the pair
+// body for every candidate, ~3.5x more work, and candidates outside the
+// support contribute exact zeros there.  Accumulators are reduced across the
+// group with xor shuffles; then one thread per target runs the per-particle
+// epilogue.
 #pragma once
 
 #include "mfree_kernels.cuh"
@@ -241,7 +243,7 @@ __device__ void epilogue(const StepArgs &a, int i, const float *res) {
             epsd = ed1;
         }
     }
-    // ---- contact reset; particles inside a tool box finish in k_finalize
+    // ---- contact reset; particles inside a tool box finish in kb_finalize
     const bool deferred = !tool && contact_candidate(a, pos.x, pos.y, pos.z);
     fc.x = fc.y = fc.z = 0.f;  // w keeps tool_p
     ft.x = ft.y = ft.z = 0.f;  // w keeps blanked
@@ -331,9 +333,6 @@ template <int LPP, int W> __host__ __device__ constexpr size_t rec_offset() {
 }
 template <int LPP, int W> __host__ __device__ constexpr int rec_capacity() {
     return int((SMEM_LIMIT - rec_offset<LPP, W>()) / (REC_N * sizeof(float4)));
-}
-__host__ __device__ inline int tile_count(const Params &P) {
-    return ((P.gnx + TX - 1) / TX) * ((P.gny + TY - 1) / TY) * ((P.gnz + P.tile_z - 1) / P.tile_z);
 }
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return unsigned(__cvta_generic_to_shared(p)); }

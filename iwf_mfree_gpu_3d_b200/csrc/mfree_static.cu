@@ -45,7 +45,7 @@ static __device__ __align__(256) StaticScratch g_static_scratch;
 constexpr int MAX_DEVICES = 64;
 StaticScratch *g_scratch_addr[MAX_DEVICES] = {nullptr};
 
-// cell hash of plain positions: the step's k_hash without blanking; a
+// cell hash of plain positions: the step's kb_hash without blanking; a
 // particle outside the grid goes to the tail like a blanked one
 __global__ void __launch_bounds__(HASH_BLOCK) k_hash_positions(StepArgs a, const float4 *pos, float bx, float by,
                                                                float bz) {
