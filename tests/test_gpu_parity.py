@@ -47,6 +47,53 @@ def test_integer_pipeline_bit_exact_every_step():
     sim.close()
 
 
+def test_integer_pipeline_bit_exact_full_size_1m():
+    """The 1,000,000-particle configuration (CSPM + PSE): cell ids, the stable
+    sort, cell ranges and neighbour counts bit-exact with the oracle's FP32
+    pipeline for 3 steps, at full size."""
+    sc = scenes.million_scene()
+    sim = _sim(sc, diagnostics=1)
+    (nx, ny, nz), bbmin, dx = sim.grid()
+    ncell = nx * ny * nz
+    for step in range(3):
+        pos_before = sim.get("POS")
+        sim.step()
+        idx = sim.get("IDX")
+        n_act, n_init = sim.counts()
+        blanked_after = sim.get("BLANKED")
+        blanked_at_hash = np.empty_like(blanked_after)
+        blanked_at_hash[idx] = blanked_after
+        h_ref = oracle.hash_fp32(pos_before, blanked_at_hash, np.array(bbmin, np.float32), dx, (nx, ny, nz))
+        idx_ref, sh_ref, cs_ref, ce_ref = oracle.sort_cells(h_ref, n_act, ncell)
+        np.testing.assert_array_equal(idx, idx_ref)
+        hsh = sim.get("HASH")
+        np.testing.assert_array_equal(hsh, sh_ref)
+        cs, ce = sim.cells()
+        np.testing.assert_array_equal(cs, cs_ref)
+        np.testing.assert_array_equal(ce, ce_ref)
+        nnb_ref = oracle.neighbor_counts_fp32(sim.get("POS_HALF"), sim.get("H"), hsh, cs, ce, n_act, (nx, ny, nz))
+        np.testing.assert_array_equal(sim.get("NUM_NBH")[:n_act], nnb_ref)
+    sim.close()
+
+
+def test_three_steps_against_fp64_oracle_full_size_1m():
+    """The 1,000,000-particle configuration against the FP64 oracle (OpenMP on
+    the host cores) after 3 steps, with the tolerances of the 100-step test."""
+    sc = scenes.million_scene()
+    sim = _sim(sc)
+    orc = oracle.Oracle(sc, prec=64)
+    for _ in range(3):
+        sim.step()
+        orc.step()
+    err = compare(gpu_state(sim), oracle_state(orc), sc)
+    print("1M, 3-step relative L2 (FP32 CUDA vs FP64 oracle):", err)
+    assert err["blank_mismatch"] == 0
+    tol = dict(POS=5e-3, VEL=5e-3, S=5e-3, EPS_PL=2e-2, T=2e-2, RHO=5e-3)
+    for k, v in tol.items():
+        assert err[k] < v, (k, err)
+    sim.close()
+
+
 def test_one_step_against_fp32_oracle():
     """One step from the same input: the CUDA path against the oracle in the
     reference's FP32 semantics.  Differences come from summation order,
