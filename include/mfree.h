@@ -45,6 +45,9 @@ extern "C" {
                                     (grid_gpu_base.cu:159-163)            */
 #define MFREE_ERR_BUDGET     -7  /* admitting the scene would exceed the
                                     batch's device-memory budget          */
+#define MFREE_ERR_TIMEOUT    -8  /* a bounded device wait ran out (the
+                                    pair kernel's staging): the step that
+                                    reported it is incomplete             */
 
 /* ---- constant records (constants_structs.h:25-92) ----------------------- */
 typedef struct { float E, nu, rho0, K, G, mass; } mfree_phys;          /* phys_constants */
@@ -119,6 +122,8 @@ typedef struct {
     int64_t contact_search_cap; /* contact shell searches stopped by the bound          */
     int64_t nan_blanked;        /* blanked particles with a NaN/Inf position or rate,
                                    summed over steps                                    */
+    int64_t staging_timeouts;   /* pair-kernel staging waits that ran out (each makes
+                                   the next call return MFREE_ERR_TIMEOUT)              */
 } mfree_counters;
 
 typedef struct mfree_ctx mfree_ctx;
@@ -224,6 +229,14 @@ int mfree_get_cells(mfree_ctx *ctx, int *cell_start, int *cell_end);
 int mfree_get_grid(const mfree_ctx *ctx, long *nx, long *ny, long *nz,
                    float *bbmin3, float *dx);
 int mfree_get_counters(mfree_ctx *ctx, mfree_counters *out);
+/* Failure injection for tests (no reference counterpart).  MFREE_FAULT_STAGING_WAIT
+ * raises the byte count the pair kernel's staging waits expect, so every wait
+ * runs out after its bound (~0.5 s), the kernel counts it and leaves, and the
+ * next call returns MFREE_ERR_TIMEOUT; nothing faults and the CUDA context
+ * stays usable.  MFREE_FAULT_NONE switches it off. */
+#define MFREE_FAULT_NONE         0
+#define MFREE_FAULT_STAGING_WAIT 1
+int mfree_inject_fault(mfree_ctx *ctx, int kind);
 
 /* ---- measurement (no reference counterpart) --------------------------------
  * Per-kernel device time of eager mfree_step calls: when on, CUDA events

@@ -44,9 +44,10 @@ EXPORTS = [
     "mfree_batch_get_tiling", "mfree_batch_autotune", "mfree_batch_sync", "mfree_batch_timer_start",
     "mfree_batch_timer_stop", "mfree_device_bytes", "mfree_scene_bytes", "mfree_write_vtk", "mfree_output_wait",
     "mfree_write_vtk_tools", "mfree_write_vtk_blanking", "mfree_append_force_log", "mfree_export_state",
-    "mfree_import_state",
+    "mfree_import_state", "mfree_inject_fault",
 ]
 ERR_BUDGET = -7
+ERR_TIMEOUT = -8
 KERNELS = ["clock", "hash", "scan_reduce", "scan_top", "scan_down", "scatter", "cell_fixup", "gather_predict",
            "interact", "finalize", "force_final"]
 
@@ -81,7 +82,7 @@ class Options(C.Structure):
 
 class Counters(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("steps", "secant_failures", "out_of_grid", "contact_search_cap",
-                                         "nan_blanked")]
+                                         "nan_blanked", "staging_timeouts")]
 
 
 _lib = None
@@ -162,6 +163,7 @@ def lib(path: str = LIB_PATH):
         getattr(L, name).argtypes = [P, C.c_char_p]
     L.mfree_output_wait.argtypes = [P]
     L.mfree_export_state.argtypes = [P, P, C.POINTER(S)]
+    L.mfree_inject_fault.argtypes = [P, I]
     L.mfree_import_state.argtypes = [P, S, P, C.POINTER(P)]
     _lib = L
     return L
@@ -372,6 +374,10 @@ class Simulation:
         ni = C.c_int()
         _check(self.L.mfree_get_counts(self.h, C.byref(n), C.byref(ni)))
         return n.value, ni.value
+
+    def inject_fault(self, kind: int):
+        """Failure injection for tests: 1 makes the pair kernel's staging waits run out, 0 clears."""
+        _check(self.L.mfree_inject_fault(self.h, int(kind)))
 
     def counters(self) -> dict:
         c = Counters()

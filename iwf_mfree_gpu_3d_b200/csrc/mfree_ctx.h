@@ -104,6 +104,7 @@ struct mfree_ctx {
     mfree_batch *owner = nullptr;
     cudaStream_t home_stream = nullptr;
     unsigned long long version = 0;
+    bool inject_staging = false;  // mfree_inject_fault: staging waits run out (tests)
     // asynchronous particle output (mfree_output.cu), created on first use
     struct OutputJob *output = nullptr;
 };

@@ -46,7 +46,7 @@ struct DevClock {
     int pending;      // 1 once a step has run: the next clock tick adds dt first
     int n_active;     // N (particles not blanked), written by the scan
     int record;       // record tool forces this step
-    int tile_error;   // staging waits that ran out (the tile fell back to global reads)
+    int staging_timeouts;  // pair-kernel staging waits that ran out (that block left its tiles undone)
     int parity;       // which of the two state copies holds this step's input (flips every step)
     long long step_index;
     float blank_min[3], blank_max[3];
@@ -100,6 +100,7 @@ struct Params {
     float tool0_vel[3];  // global_tool[0]->get_vel(): friction heat and tool particles
     int record_every;
     int tile_z;  // cells per pair-kernel tile along z (1..TILE_Z_MAX)
+    int stage_extra;  // bytes added to the staging byte count: nonzero only to make the waits run out (tests)
 };
 
 struct State {

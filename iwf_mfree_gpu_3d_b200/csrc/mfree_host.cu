@@ -10,6 +10,7 @@
 // A step is 11 kernels on one stream with no host synchronisation (N lives on
 // the device), so it can also be captured once into a CUDA graph and replayed.
 #include <climits>
+#include <cstddef>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -125,6 +126,7 @@ Params make_params(const mfree_ctx *c) {
     for (int d = 0; d < 3; d++) P.tool0_vel[d] = c->tools.empty() ? 0.f : c->tools[0]->vel[d];
     P.record_every = 0;
     P.tile_z = c->opt.tile_depth > 0 ? c->opt.tile_depth : default_tile_depth();
+    P.stage_extra = c->inject_staging ? 16 : 0;
     return P;
 }
 
@@ -211,6 +213,7 @@ int write_clock(mfree_ctx *c) {
     h.out_of_grid = old.out_of_grid;
     h.contact_cap = old.contact_cap;
     h.nan_blanked = old.nan_blanked;
+    h.staging_timeouts = old.staging_timeouts;
     h.n_active = old.n_active ? old.n_active : c->n_init;
     CUDA_TRY(cudaMemcpyAsync(c->d_clk, &h, sizeof(DevClock), cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -357,16 +360,21 @@ int check_empty(mfree_ctx *c, bool wait) {
     if (!wait && cudaEventQuery(c->nact_ev) != cudaSuccess) return MFREE_OK;
     CUDA_TRY(cudaEventSynchronize(c->nact_ev));
     c->nact_pending = false;
-    if (*c->h_nact == 0) return fail(MFREE_ERR_EMPTY, "all particles are blanked (outside the blanking box)");
+    if (c->h_nact[2] > 0)
+        return fail(MFREE_ERR_TIMEOUT, "a staging wait of the pair kernel ran out: the step is incomplete (" +
+                                           std::to_string(c->h_nact[2]) + " waits)");
+    if (c->h_nact[0] == 0) return fail(MFREE_ERR_EMPTY, "all particles are blanked (outside the blanking box)");
     return MFREE_OK;
 }
 
 int note_active_count(mfree_ctx *c) {
     if (!c->h_nact) {
-        CUDA_TRY(cudaMallocHost(&c->h_nact, sizeof(int)));
+        CUDA_TRY(cudaMallocHost(&c->h_nact, 3 * sizeof(int)));
         CUDA_TRY(cudaEventCreateWithFlags(&c->nact_ev, cudaEventDisableTiming));
     }
-    CUDA_TRY(cudaMemcpyAsync(c->h_nact, &c->d_clk->n_active, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    // n_active, record, staging_timeouts: adjacent in the device clock
+    static_assert(offsetof(DevClock, staging_timeouts) == offsetof(DevClock, n_active) + 2 * sizeof(int), "clock layout");
+    CUDA_TRY(cudaMemcpyAsync(c->h_nact, &c->d_clk->n_active, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaEventRecord(c->nact_ev, c->stream));
     c->nact_pending = true;
     return MFREE_OK;
@@ -917,6 +925,14 @@ int mfree_get_counts(const mfree_ctx *c, int *n_active, int *n_init) {
     return MFREE_OK;
 }
 
+int mfree_inject_fault(mfree_ctx *c, int kind) {
+    if (!c) return fail(MFREE_ERR_ARG, "null context");
+    if (kind != MFREE_FAULT_NONE && kind != MFREE_FAULT_STAGING_WAIT) return fail(MFREE_ERR_ARG, "unknown fault kind");
+    c->inject_staging = kind == MFREE_FAULT_STAGING_WAIT;
+    invalidate_graphs(c);  // the step arguments change
+    return MFREE_OK;
+}
+
 int mfree_get_counters(mfree_ctx *c, mfree_counters *o) {
     if (!c || !o) return fail(MFREE_ERR_ARG, "null argument");
     DevClock h{};
@@ -927,6 +943,7 @@ int mfree_get_counters(mfree_ctx *c, mfree_counters *o) {
     o->out_of_grid = int64_t(h.out_of_grid);
     o->contact_search_cap = int64_t(h.contact_cap);
     o->nan_blanked = int64_t(h.nan_blanked);
+    o->staging_timeouts = int64_t(h.staging_timeouts);
     return MFREE_OK;
 }
 

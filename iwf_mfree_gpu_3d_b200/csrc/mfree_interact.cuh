@@ -306,6 +306,7 @@ template <bool CSPM> __host__ __device__ constexpr int tile_threads() { return 6
 constexpr int TCAP = 320;              // targets per pass of a tile
 constexpr int QCAP_T = 96;             // in-support queue per target before the rescan path
 constexpr int SMEM_LIMIT = 232448;     // per-block shared memory of sm_100
+constexpr long long WAIT_CYCLES = 1ll << 30;  // bound of a staging wait (~0.5 s of SM clock)
 
 template <int LPP, int TILE_WARPS> struct TileSmem {
     static constexpr int G = 32 / LPP;
@@ -643,7 +644,8 @@ __device__ __forceinline__ bool interact_tile(const StepArgs &a, TileSmem<LPP, t
             if (lane == 0) {
                 sm.total = tot;
                 sm.staged = tot <= CAP ? 1 : 0;
-                if (sm.staged && tot > 0) mbar_expect(&sm.bar, unsigned(tot) * unsigned(REC_N * sizeof(float4)));
+                if (sm.staged && tot > 0)
+                    mbar_expect(&sm.bar, unsigned(tot) * unsigned(REC_N * sizeof(float4)) + unsigned(P.stage_extra));
             }
         }
         __syncthreads();
@@ -658,20 +660,21 @@ __device__ __forceinline__ bool interact_tile(const StepArgs &a, TileSmem<LPP, t
                                  unsigned(len) * unsigned(sizeof(float4)), &sm.bar);
             }
             const unsigned par = unsigned(sm.parity);
-            unsigned it = 0;
+            const long long t_wait = clock64();
             bool ok = true;
             while (!mbar_try(&sm.bar, par)) {
-                if (++it > (1u << 22)) {
+                if (clock64() - t_wait > WAIT_CYCLES) {
                     ok = false;
                     break;
                 }
             }
             if (!__syncthreads_and(ok)) {
-                // the copies did not complete in time: record it, wait once more
-                // (bounded) for them to land, and leave the kernel
-                if (threadIdx.x == 0) atomicAdd(&a.clk->tile_error, 1);
-                unsigned it2 = 0;
-                while (!mbar_try(&sm.bar, par) && ++it2 < (1u << 22)) {
+                // the copies did not complete in time: count it (the host
+                // reports MFREE_ERR_TIMEOUT), wait once more (bounded) for the
+                // copies in flight to land, and leave the kernel
+                if (threadIdx.x == 0) atomicAdd(&a.clk->staging_timeouts, 1);
+                const long long t2 = clock64();
+                while (!mbar_try(&sm.bar, par) && clock64() - t2 <= WAIT_CYCLES) {
                 }
                 return false;
             }
