@@ -522,41 +522,29 @@ int mfree_create(int n, const float *pos4, const float *vel4, const float *rho, 
     std::unique_ptr<mfree_ctx> c;
     int st = alloc_ctx(n, (cudaStream_t)stream, c);
     if (st) return st;
-    // initial state, reference constructor semantics (zeros except the given fields)
-    std::vector<float4> hp(n), hv(n), hz(n, make_float4(0, 0, 0, 0)), hsb(n), hdsb(n), hfc(n), hft(n), hbc(n);
-    std::vector<int> perm(n);
-    for (int i = 0; i < n; i++) {
-        hp[i] = make_float4(pos4[4 * i], pos4[4 * i + 1], pos4[4 * i + 2], h[i]);
-        hv[i] = make_float4(vel4[4 * i], vel4[4 * i + 1], vel4[4 * i + 2], rho[i]);
-        hsb[i] = make_float4(0.f, 0.f, T ? T[i] : 0.f, 0.f);
-        hdsb[i] = make_float4(0.f, 0.f, 0.f, fixed ? fixed[i] : 0.f);
-        hfc[i] = make_float4(0.f, 0.f, 0.f, tool_p ? tool_p[i] : 0.f);
-        hft[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        int id = i;
-        float idf;
-        std::memcpy(&idf, &id, 4);
-        hbc[i] = make_float4(0.f, 0.f, 0.f, idf);
-        perm[i] = i;
+    // the caller's arrays go to the device as they are (staged in the record
+    // buffer, which the first step overwrites) and a kernel builds the state:
+    // the reference constructor's semantics, zeros except the given fields
+    {
+        float *stage = reinterpret_cast<float *>(c->rec.f[0]);  // REC_N * 4 floats per particle >= 8 + 5 here
+        const size_t nn = size_t(n);
+        float *d_pos = stage, *d_vel = stage + 4 * nn, *d_rho = stage + 8 * nn, *d_h = stage + 9 * nn;
+        float *d_T = T ? stage + 10 * nn : nullptr, *d_fix = fixed ? stage + 11 * nn : nullptr,
+              *d_tool = tool_p ? stage + 12 * nn : nullptr;
+        auto up = [&](float *d, const float *hsrc, size_t count) {
+            return cudaMemcpyAsync(d, hsrc, sizeof(float) * count, cudaMemcpyHostToDevice, c->stream);
+        };
+        CUDA_TRY(up(d_pos, pos4, 4 * nn));
+        CUDA_TRY(up(d_vel, vel4, 4 * nn));
+        CUDA_TRY(up(d_rho, rho, nn));
+        CUDA_TRY(up(d_h, h, nn));
+        if (T) CUDA_TRY(up(d_T, T, nn));
+        if (fixed) CUDA_TRY(up(d_fix, fixed, nn));
+        if (tool_p) CUDA_TRY(up(d_tool, tool_p, nn));
+        CUDA_TRY(launch_init_state(n, reinterpret_cast<const float4 *>(d_pos), reinterpret_cast<const float4 *>(d_vel),
+                                   d_rho, d_T, d_h, d_fix, d_tool, c->st[0], c->scr.perm, c->stream));
     }
-    State &S = c->st[0];
-    auto up = [&](float4 *d, const std::vector<float4> &v) {
-        return cudaMemcpyAsync(d, v.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, c->stream);
-    };
-    CUDA_TRY(up(S.pos4, hp));
-    CUDA_TRY(up(S.vel4, hv));
-    CUDA_TRY(up(S.sa4, hz));
-    CUDA_TRY(up(S.sb4, hsb));
-    CUDA_TRY(up(S.da4, hz));
-    CUDA_TRY(up(S.dv4, hz));
-    CUDA_TRY(up(S.dsa4, hz));
-    CUDA_TRY(up(S.dsb4, hdsb));
-    CUDA_TRY(up(S.fc4, hfc));
-    CUDA_TRY(up(S.ft4, hft));
-    CUDA_TRY(up(S.bc4, hbc));
-    CUDA_TRY(up(S.lo4, hz));
-    CUDA_TRY(up(S.lo4b, hz));
     CUDA_TRY(cudaMemsetAsync(c->rec.f[0], 0, sizeof(float4) * REC_N * n, c->stream));
-    CUDA_TRY(cudaMemcpyAsync(c->scr.perm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(cudaMemsetAsync(c->scr.key_sorted, 0, sizeof(int) * n, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     *out = c.release();

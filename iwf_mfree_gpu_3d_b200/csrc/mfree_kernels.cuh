@@ -129,6 +129,11 @@ __global__ void k_scan_down(StepArgs a);
 __global__ void k_scatter(StepArgs a);
 __global__ void k_cell_fixup(StepArgs a);
 
+// initial particle state from the constructor's device arrays (mfree_create)
+cudaError_t launch_init_state(int n, const float4 *pos, const float4 *vel, const float *rho, const float *T,
+                              const float *h, const float *fixed, const float *tool_p, const State &S, int *perm,
+                              cudaStream_t s);
+
 // message returned by mfree_last_error() (mfree_host.cu)
 void set_last_error(const std::string &msg);
 

@@ -340,6 +340,39 @@ template <bool PREC> __global__ void __launch_bounds__(256) kb_gather_predict(Ba
     run_batched(T, T.pblk, [](const StepArgs &a, int b) { gather_predict_body<PREC>(a, b); });
 }
 
+// the initial state of a context from the constructor's arrays (particle_gpu,
+// particle_gpu.cu:20-117: zeros except the given fields); the optional arrays
+// may be NULL
+__global__ void __launch_bounds__(256) k_init_state(int n, const float4 *pos, const float4 *vel, const float *rho,
+                                                    const float *T, const float *h, const float *fixed,
+                                                    const float *tool_p, State S, int *perm) {
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= n) return;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 p = pos[i], v = vel[i];
+    S.pos4[i] = make_float4(p.x, p.y, p.z, h[i]);
+    S.vel4[i] = make_float4(v.x, v.y, v.z, rho[i]);
+    S.sa4[i] = z;
+    S.sb4[i] = make_float4(0.f, 0.f, T ? T[i] : 0.f, 0.f);
+    S.da4[i] = z;
+    S.dv4[i] = z;
+    S.dsa4[i] = z;
+    S.dsb4[i] = make_float4(0.f, 0.f, 0.f, fixed ? fixed[i] : 0.f);
+    S.fc4[i] = make_float4(0.f, 0.f, 0.f, tool_p ? tool_p[i] : 0.f);
+    S.ft4[i] = z;
+    S.bc4[i] = make_float4(0.f, 0.f, 0.f, __int_as_float(i));  // creation index
+    S.lo4[i] = z;
+    S.lo4b[i] = z;
+    perm[i] = i;
+}
+
+cudaError_t launch_init_state(int n, const float4 *pos, const float4 *vel, const float *rho, const float *T,
+                              const float *h, const float *fixed, const float *tool_p, const State &S, int *perm,
+                              cudaStream_t s) {
+    k_init_state<<<(n + 255) / 256, 256, 0, s>>>(n, pos, vel, rho, T, h, fixed, tool_p, S, perm);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_gather_predict_batch(const BatchTable &T, bool precision, int blocks, cudaStream_t s) {
     if (precision) kb_gather_predict<true><<<blocks, 256, 0, s>>>(T);
     else kb_gather_predict<false><<<blocks, 256, 0, s>>>(T);
