@@ -448,10 +448,11 @@ def run_serve(args, tiling) -> dict:
 def run_e2e(sc, args, opts, dist, local_rank) -> dict:
     """The same metric through the C ABI from pinned host buffers: the particle
     arrays are uploaded (mfree_create, as the reference's particle_gpu
-    constructor), every step records and reads back the tool force (as the
-    reference's driver does on its output steps), and the state the user reads
-    (position, velocity, stress, temperature, plastic strain) is copied back at
-    the end; wall clock around all of it."""
+    constructor), every step (one replay of the captured step) records and
+    reads back the tool force (as the reference's driver does on its output
+    steps), and the state the user reads (position, velocity, stress,
+    temperature, plastic strain) is copied back at the end; wall clock around
+    all of it."""
     from iwf_mfree_gpu_3d_b200 import api
     import torch
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
@@ -483,8 +484,8 @@ def run_e2e(sc, args, opts, dist, local_rank) -> dict:
     s.set_time(float(dt), float(dt))
     d2h = 0
     for _ in range(args.steps):
-        s.step(record_forces=True)
-        f = s.tool_forces()
+        s.advance(1, record_every=1, use_graph=True)  # one replay of the captured step, forces recorded
+        f = s.tool_forces()  # the step's result, read back every step
         d2h += f.nbytes
     out = [s.get(n) for n in ("POS", "VEL", "S", "T", "EPS_PL")]
     d2h += sum(a.nbytes for a in out)
