@@ -29,7 +29,10 @@
 // body for every candidate, ~3.5x more work, and candidates outside the
 // support contribute exact zeros there.  Accumulators are reduced across the
 // group with xor shuffles; then one thread per target runs the per-particle
-// epilogue.
+// epilogue.  The epilogue needs at most TCAP = 320 threads; during the
+// epilogue of a tile's last pass the other 320 already prepare the next tile
+// (its target ranges, halo table and staging copies), so those copies land
+// while the epilogue runs.
 #pragma once
 
 #include "mfree_kernels.cuh"
@@ -323,6 +326,8 @@ template <int LPP, int TILE_WARPS> struct TileSmem {
     int tpref[NTC + 1];
     unsigned long long bar;
     int tile, total, staged, parity, scene;
+    int next_args;     // scene whose arguments the second args buffer holds (-1: none)
+    int ntile, nscene; // the prologue threads' candidate tile
 };
 __host__ __device__ constexpr size_t round128(size_t b) { return (b + 127) / 128 * 128; }
 // shared memory: the tables, the scene's arguments, the staged records
@@ -330,7 +335,7 @@ template <int LPP, int W> __host__ __device__ constexpr size_t args_offset() {
     return round128(sizeof(TileSmem<LPP, W>));
 }
 template <int LPP, int W> __host__ __device__ constexpr size_t rec_offset() {
-    return args_offset<LPP, W>() + round128(sizeof(StepArgs));
+    return args_offset<LPP, W>() + 2 * round128(sizeof(StepArgs));  // the current and the next tile's scene
 }
 template <int LPP, int W> __host__ __device__ constexpr int rec_capacity() {
     return int((SMEM_LIMIT - rec_offset<LPP, W>()) / (REC_N * sizeof(float4)));
@@ -573,39 +578,77 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
     __syncwarp();
 }
 
-// one tile of the cell grid: target ranges (an empty tile ends there), halo
-// cell starts, staging, then the targets in passes of TCAP.  Returns false
-// when a staging wait ran out (the caller leaves the kernel).
-template <int LPP, bool CSPM, int COND, bool PREC, int CAP>
-__device__ __forceinline__ bool interact_tile(const StepArgs &a, TileSmem<LPP, tile_threads<CSPM>() / 32> &sm,
-                                              float4 *sarr, int tile) {
-    constexpr int TILE_THREADS = tile_threads<CSPM>();
-    constexpr int TILE_WARPS = TILE_THREADS / 32;
-    constexpr int G = 32 / LPP;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int g = lane / LPP, sl = lane - g * LPP;
-    const Params &P = a.p;
-    const int nx = P.gnx, ny = P.gny, nz = P.gnz;
+// threads at or above PRO_FIRST never run the epilogue (TCAP <= PRO_FIRST):
+// while the others finish the current tile, they prepare the next one
+constexpr int PRO_FIRST = TCAP;
+__device__ __forceinline__ void pro_sync(int nthreads) { asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory"); }
+
+struct TileGeo {
+    int X0, Y0, Z0, zl, nzr;
+};
+__device__ __forceinline__ TileGeo tile_geo(const Params &P, int t) {
     const int TZ = P.tile_z;
-    const int nty = (ny + TY - 1) / TY, ntz = (nz + TZ - 1) / TZ;
-    const int *__restrict__ first = a.s.first;
-    const float4 *gbase = a.r.f[0];  // the record arrays are one allocation: f[k] = f[0] + k * n_init
-    const int gstride = P.n_init;
-    {
-        const int tz = tile % ntz, txy = tile / ntz, ty = txy % nty, tx = txy / nty;
-        const int X0 = tx * TX, Y0 = ty * TY, Z0 = tz * TZ;
-        const int zl = max(Z0 - 2, 0), zh = min(Z0 + TZ + 1, nz - 1);
-        const int nzr = zh - zl + 2;  // cell starts per halo column (inclusive end)
-        // ---- target column ranges first: empty tiles end here
-        if (threadIdx.x < 32) {
-            const int c = threadIdx.x;
+    const int nty = (P.gny + TY - 1) / TY, ntz = (P.gnz + TZ - 1) / TZ;
+    const int tz = t % ntz, txy = t / ntz, ty = txy % nty, tx = txy / nty;
+    TileGeo g;
+    g.X0 = tx * TX;
+    g.Y0 = ty * TY;
+    g.Z0 = tz * TZ;
+    g.zl = max(g.Z0 - 2, 0);
+    g.nzr = min(g.Z0 + TZ + 1, P.gnz - 1) - g.zl + 2;  // cell starts per halo column (inclusive end)
+    return g;
+}
+
+// Run by the prologue threads: pulls tiles from the queue until a non-empty
+// one (or none is left), copies its scene's arguments into the second args
+// buffer when the scene is not the current tile's (busy_scene), builds its
+// target ranges, halo cell starts and halo offsets, and issues its staging
+// copies.  The prepared tile is left in sm.tile / sm.scene (tile = total:
+// none left).  The caller guarantees that nothing reads the staged records or
+// the tile tables any more.  Kept out of line: inlined into the kernel's loop
+// it made the pair rounds about 7% slower (measured on the 1M-particle step).
+template <int LPP, int W, int CAP>
+__device__ __noinline__ void prepare_tile(const BatchTable &T, TileSmem<LPP, W> &sm, StepArgs *sa, float4 *sarr,
+                                          int total, int busy_scene) {
+    constexpr int PT = W * 32 - PRO_FIRST;
+    const int ptid = threadIdx.x - PRO_FIRST, pl = ptid & 31, pw = ptid >> 5;
+    for (;;) {
+        if (ptid == 0) {
+            const int t = atomicAdd(T.tile_next, 1);
+            sm.ntile = t;
+            sm.nscene = t < total ? find_scene(T.itile, T.nscenes, t) : -1;
+        }
+        pro_sync(PT);
+        const int t = sm.ntile, s = sm.nscene;
+        if (t >= total) {
+            if (ptid == 0) sm.tile = total;
+            return;
+        }
+        // another scene's arguments go to the second buffer (the current
+        // tile's, in the first, are in use); the main loop moves them over
+        const int buf = s == busy_scene ? 0 : 1;
+        if (buf == 1 && sm.next_args != s) {
+            const StepArgs *a0 = T.args + 2 * s;
+            const int4 *src = reinterpret_cast<const int4 *>(a0 + (a0->clk->parity & 1));
+            int4 *d = reinterpret_cast<int4 *>(sa + 1);
+            for (int k = ptid; k < int(sizeof(StepArgs) / 16); k += PT) d[k] = src[k];
+            pro_sync(PT);
+            if (ptid == 0) sm.next_args = s;
+        }
+        const StepArgs &a = sa[buf];
+        const Params &P = a.p;
+        const int nx = P.gnx, ny = P.gny, nz = P.gnz;
+        const TileGeo G = tile_geo(P, t - T.itile[s]);
+        const int *__restrict__ first = a.s.first;
+        if (pw == 0) {  // target column ranges: an empty tile ends here
+            const int c = pl;
             int s0 = 0, len = 0;
             if (c < NTC) {
-                const int cx = X0 + c / TY, cy = Y0 + c % TY;
-                if (cx < nx && cy < ny && Z0 < nz) {
+                const int cx = G.X0 + c / TY, cy = G.Y0 + c % TY;
+                if (cx < nx && cy < ny && G.Z0 < nz) {
                     const int cb = (cx * ny + cy) * nz;
-                    s0 = first[cb + Z0];
-                    len = first[cb + min(Z0 + TZ - 1, nz - 1) + 1] - s0;
+                    s0 = first[cb + G.Z0];
+                    len = first[cb + min(G.Z0 + P.tile_z - 1, nz - 1) + 1] - s0;
                 }
                 sm.tstart[c] = s0;
             }
@@ -613,52 +656,123 @@ __device__ __forceinline__ bool interact_tile(const StepArgs &a, TileSmem<LPP, t
             if (c < NTC) sm.tpref[c] = ti - len;
             if (c == 31) sm.tpref[NTC] = ti;
         }
-        __syncthreads();
-        if (sm.tpref[NTC] == 0) return true;  // (the caller's loop head synchronises before the next tile)
-        // ---- halo cell starts
-        for (int e = threadIdx.x; e < NHC * CSROW; e += TILE_THREADS) {
-            const int c = e / CSROW, k = e - c * CSROW;
-            const int cx = X0 - 2 + c / HY, cy = Y0 - 2 + c % HY;
-            int v = 0;
-            if (k < nzr && cx >= 0 && cx < nx && cy >= 0 && cy < ny) v = first[(cx * ny + cy) * nz + zl + k];
-            sm.cellstart[c][k] = v;
+        pro_sync(PT);
+        if (sm.tpref[NTC] == 0) continue;
+        {  // halo cell starts, each thread's loads in flight together
+            constexpr int NCS = (NHC * CSROW + PT - 1) / PT;
+            int csv[NCS];
+#pragma unroll
+            for (int r = 0; r < NCS; r++) {
+                const int e = ptid + r * PT;
+                const int c = e / CSROW, k = e - c * CSROW;
+                const int cx = G.X0 - 2 + c / HY, cy = G.Y0 - 2 + c % HY;
+                csv[r] = 0;
+                if (e < NHC * CSROW && k < G.nzr && cx >= 0 && cx < nx && cy >= 0 && cy < ny)
+                    csv[r] = first[(cx * ny + cy) * nz + G.zl + k];
+            }
+#pragma unroll
+            for (int r = 0; r < NCS; r++) {
+                const int e = ptid + r * PT;
+                if (e < NHC * CSROW) (&sm.cellstart[0][0])[e] = csv[r];
+            }
         }
-        __syncthreads();
-        if (warp == 0) {  // prefix sum of the 64 halo columns; staging decision
+        pro_sync(PT);
+        if (pw == 0) {  // prefix sum of the 64 halo columns; staging decision
             int len2[2];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-                const int c = lane + 32 * h;
-                const int cx = X0 - 2 + c / HY, cy = Y0 - 2 + c % HY;
+                const int c = pl + 32 * h;
+                const int cx = G.X0 - 2 + c / HY, cy = G.Y0 - 2 + c % HY;
                 const bool in = cx >= 0 && cx < nx && cy >= 0 && cy < ny;
-                len2[h] = in ? sm.cellstart[c][nzr - 1] - sm.cellstart[c][0] : 0;
+                len2[h] = in ? sm.cellstart[c][G.nzr - 1] - sm.cellstart[c][0] : 0;
                 sm.hstart[c] = sm.cellstart[c][0];
                 sm.hlen[c] = len2[h];
             }
-            const int i0 = group_scan<32>(len2[0], lane);
+            const int i0 = group_scan<32>(len2[0], pl);
             const int t0 = __shfl_sync(0xffffffffu, i0, 31);
-            const int i1 = group_scan<32>(len2[1], lane);
-            sm.hoff[lane] = i0 - len2[0];
-            sm.hoff[lane + 32] = t0 + i1 - len2[1];
+            const int i1 = group_scan<32>(len2[1], pl);
+            sm.hoff[pl] = i0 - len2[0];
+            sm.hoff[pl + 32] = t0 + i1 - len2[1];
             const int tot = t0 + __shfl_sync(0xffffffffu, i1, 31);
-            if (lane == 0) {
+            if (pl == 0) {
                 sm.total = tot;
                 sm.staged = tot <= CAP ? 1 : 0;
                 if (sm.staged && tot > 0)
                     mbar_expect(&sm.bar, unsigned(tot) * unsigned(REC_N * sizeof(float4)) + unsigned(P.stage_extra));
             }
         }
-        __syncthreads();
-        const int T = sm.tpref[NTC];
-        const bool staged = sm.staged != 0;
-        if (staged && sm.total > 0) {
-            if (threadIdx.x < REC_N * NHC) {
-                const int k = threadIdx.x / NHC, c = threadIdx.x - k * NHC;
+        pro_sync(PT);
+        if (sm.staged && sm.total > 0) {
+            const float4 *gbase = a.r.f[0];  // the record arrays are one allocation: f[k] = f[0] + k * n_init
+            for (int q = ptid; q < REC_N * NHC; q += PT) {
+                const int k = q / NHC, c = q - k * NHC;
                 const int len = sm.hlen[c];
                 if (len > 0)
-                    bulk_to_smem(sarr + k * CAP + sm.hoff[c], gbase + size_t(k) * gstride + sm.hstart[c],
+                    bulk_to_smem(sarr + k * CAP + sm.hoff[c], gbase + size_t(k) * P.n_init + sm.hstart[c],
                                  unsigned(len) * unsigned(sizeof(float4)), &sm.bar);
             }
+        }
+        if (ptid == 0) {
+            sm.tile = t;
+            sm.scene = s;
+        }
+        return;
+    }
+}
+
+template <class SM> __device__ __forceinline__ void init_tile_smem(SM &sm) {
+    if (threadIdx.x == 0) {
+        mbar_init(&sm.bar, 1);
+        sm.parity = 0;
+        sm.next_args = -1;
+    }
+    fence_proxy_async();
+    __syncthreads();
+}
+
+// Persistent (one block per SM) over the tiles of every scene of the table
+// (one queue).  Per tile: wait for its staged halo, then the targets in passes
+// of TCAP (rounds of all warps, then the epilogue by the threads below
+// PRO_FIRST); during the last pass's epilogue the threads from PRO_FIRST on
+// already prepare the next tile and start its staging copies.
+template <int LPP, bool CSPM, int COND, bool PREC>
+__global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTable T) {
+    constexpr int TILE_THREADS = tile_threads<CSPM>();
+    constexpr int TILE_WARPS = TILE_THREADS / 32;
+    constexpr int W = TILE_WARPS;
+    constexpr int CAP = rec_capacity<LPP, W>();
+    constexpr int G = 32 / LPP;
+    static_assert(TILE_THREADS - PRO_FIRST >= 64, "the prologue needs two warps at least");
+    extern __shared__ __align__(128) unsigned char dyn[];
+    TileSmem<LPP, W> &sm = *reinterpret_cast<TileSmem<LPP, W> *>(dyn);
+    StepArgs *sa = reinterpret_cast<StepArgs *>(dyn + args_offset<LPP, W>());
+    float4 *sarr = reinterpret_cast<float4 *>(dyn + rec_offset<LPP, W>());
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane / LPP, sl = lane - g * LPP;
+    init_tile_smem(sm);
+    const int total = T.itile[T.nscenes];
+    int cur = -1;
+    if (threadIdx.x >= PRO_FIRST) prepare_tile<LPP, W, CAP>(T, sm, sa, sarr, total, cur);
+    const StepArgs &a = sa[0];
+    for (;;) {
+        __syncthreads();  // the prepared tile's descriptor and tables are visible
+        const int tile = sm.tile;
+        if (tile >= total) break;
+        const int s = sm.scene;
+        if (s != cur) {  // a new scene: its arguments wait in the second buffer
+            const int4 *src = reinterpret_cast<const int4 *>(sa + 1);
+            int4 *d = reinterpret_cast<int4 *>(sa);
+            for (int k = threadIdx.x; k < int(sizeof(StepArgs) / 16); k += blockDim.x) d[k] = src[k];
+            __syncthreads();
+            cur = s;
+        }
+        const TileGeo geo = tile_geo(a.p, tile - T.itile[s]);
+        const int X0 = geo.X0, Y0 = geo.Y0, zl = geo.zl;
+        const float4 *gbase = a.r.f[0];
+        const int gstride = a.p.n_init;
+        const int ntg = sm.tpref[NTC];
+        const bool staged = sm.staged != 0;
+        if (staged && sm.total > 0) {
             const unsigned par = unsigned(sm.parity);
             const long long t_wait = clock64();
             bool ok = true;
@@ -676,13 +790,13 @@ __device__ __forceinline__ bool interact_tile(const StepArgs &a, TileSmem<LPP, t
                 const long long t2 = clock64();
                 while (!mbar_try(&sm.bar, par) && clock64() - t2 <= WAIT_CYCLES) {
                 }
-                return false;
+                return;
             }
             if (threadIdx.x == 0) sm.parity ^= 1;
         }
-        // ---- targets, TCAP per pass
-        for (int t0 = 0; t0 < T; t0 += TCAP) {
-            const int tn = min(TCAP, T - t0);
+        for (int t0 = 0; t0 < ntg; t0 += TCAP) {
+            const int tn = min(TCAP, ntg - t0);
+            const bool last = t0 + TCAP >= ntg;
             for (int tt = threadIdx.x; tt < tn; tt += TILE_THREADS) {
                 const int tg = t0 + tt;
                 int c = 0;
@@ -732,58 +846,18 @@ __device__ __forceinline__ bool interact_tile(const StepArgs &a, TileSmem<LPP, t
                     done += TILE_WARPS * G;
                 }
             }
-            // the rounds were the last generic reads of the staged halo: order
-            // them before the next tile's bulk writes (the barriers that follow
-            // carry the order to the threads that issue the copies)
+            // the rounds were the last generic reads of the staged halo and the
+            // tile tables: order them before the next tile's bulk writes, which
+            // the prologue threads issue after this barrier
             fence_proxy_async();
             __syncthreads();
-            // ---- per-particle rest of the step, one thread per target
-            for (int tt = threadIdx.x; tt < tn; tt += TILE_THREADS) epilogue<PREC, COND>(a, sm.tgt[tt], sm.res[tt]);
-            __syncthreads();
+            if (threadIdx.x < PRO_FIRST) {
+                if (threadIdx.x < tn) epilogue<PREC, COND>(a, sm.tgt[threadIdx.x], sm.res[threadIdx.x]);
+            } else if (last) {
+                prepare_tile<LPP, W, CAP>(T, sm, sa, sarr, total, s);
+            }
+            if (!last) __syncthreads();
         }
-    }
-    return true;
-}
-
-template <class SM> __device__ __forceinline__ void init_tile_smem(SM &sm) {
-    if (threadIdx.x == 0) {
-        mbar_init(&sm.bar, 1);
-        sm.parity = 0;
-    }
-    fence_proxy_async();
-    __syncthreads();
-}
-
-// persistent (one block per SM) over the tiles of every scene of the table
-// (one queue); a block copies a scene's arguments into shared memory when its
-// next tile belongs to another scene than its last one
-template <int LPP, bool CSPM, int COND, bool PREC>
-__global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTable T) {
-    constexpr int W = tile_threads<CSPM>() / 32;
-    constexpr int CAP = rec_capacity<LPP, W>();
-    extern __shared__ __align__(128) unsigned char dyn[];
-    TileSmem<LPP, W> &sm = *reinterpret_cast<TileSmem<LPP, W> *>(dyn);
-    StepArgs &sa = *reinterpret_cast<StepArgs *>(dyn + args_offset<LPP, W>());
-    float4 *sarr = reinterpret_cast<float4 *>(dyn + rec_offset<LPP, W>());
-    init_tile_smem(sm);
-    const int total = T.itile[T.nscenes];
-    int cur = -1;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            const int t = atomicAdd(T.tile_next, 1);
-            sm.tile = t;
-            sm.scene = t < total ? find_scene(T.itile, T.nscenes, t) : -1;
-        }
-        __syncthreads();
-        const int tile = sm.tile;
-        if (tile >= total) break;
-        const int s = sm.scene;
-        if (s != cur) {  // every thread has finished the last tile (barriers at its end)
-            load_scene_args(sa, T, s);
-            __syncthreads();
-            cur = s;
-        }
-        if (!interact_tile<LPP, CSPM, COND, PREC, CAP>(sa, sm, sarr, tile - T.itile[s])) return;
     }
 }
 
