@@ -53,6 +53,8 @@ struct mfree_batch {
     // device table: StepArgs[2 cap] | 4 prefixes of cap + 1 ints | queue counter
     void *d_table = nullptr;
     int cap = 0;
+    int2 *d_tiles = nullptr;  // the pair kernel's tile list over every scene
+    int tiles_cap = 0;
     BatchTable T{};
     std::vector<int> run;  // slots in the table, in table order
     int tot_pblk = 0, tot_stile = 0, tot_cblk = 0, tot_itile = 0;
@@ -65,7 +67,7 @@ struct mfree_batch {
 namespace {
 
 size_t table_bytes(int cap) {
-    return sizeof(StepArgs) * 2 * size_t(cap) + sizeof(int) * (4 * size_t(cap + 1) + 1);
+    return sizeof(StepArgs) * 2 * size_t(cap) + sizeof(int) * (4 * size_t(cap + 1) + 2);
 }
 
 void drop_graph(mfree_batch *b) {
@@ -103,6 +105,7 @@ int build_table(mfree_batch *b, int record_every) {
     b->T.cblk = dint + 2 * (b->cap + 1);
     b->T.itile = dint + 3 * (b->cap + 1);
     b->T.tile_next = dint + 4 * (b->cap + 1);
+    b->T.tile_count = dint + 4 * (b->cap + 1) + 1;
     std::vector<StepArgs> args(2 * size_t(n));
     std::vector<int> pre(4 * size_t(b->cap + 1), 0);
     int *pb = pre.data(), *ps = pb + (b->cap + 1), *pc = ps + (b->cap + 1), *pt = pc + (b->cap + 1);
@@ -129,12 +132,22 @@ int build_table(mfree_batch *b, int record_every) {
         pb[s + 1] = pb[s] + hash_blocks(c);
         ps[s + 1] = ps[s] + scan_tiles(c);
         pc[s + 1] = pc[s] + int((c->num_cell + 255) / 256);
-        pt[s + 1] = pt[s] + ((P.gnx + 3) / 4) * ((P.gny + 3) / 4) * ((P.gnz + P.tile_z - 1) / P.tile_z);
+        pt[s + 1] = pt[s] + num_tiles(P);
     }
     b->tot_pblk = pb[n];
     b->tot_stile = ps[n];
     b->tot_cblk = pc[n];
     b->tot_itile = pt[n];
+    if (b->tot_itile > b->tiles_cap) {  // the tile list of all scenes
+        CUDA_TRY(cudaStreamSynchronize(b->stream));  // the old list may still be read
+        const int cap = std::max(b->tot_itile, 2 * b->tiles_cap);
+        if (b->d_tiles) cudaFree(b->d_tiles);
+        b->d_tiles = nullptr;
+        b->tiles_cap = 0;
+        CUDA_TRY(cudaMalloc(&b->d_tiles, sizeof(int2) * size_t(cap)));
+        b->tiles_cap = cap;
+    }
+    b->T.tile_list = b->d_tiles;
     // pageable sources: the call returns once the bytes are staged, so the
     // vectors may go; the device copy stays ordered on the stream
     CUDA_TRY(cudaMemcpyAsync(dargs, args.data(), sizeof(StepArgs) * args.size(), cudaMemcpyHostToDevice, b->stream));
@@ -156,7 +169,7 @@ int enqueue_batch_step(mfree_batch *b, int record_mode) {
     kb_scan_top<<<n, 1024, 0, s>>>(T);
     kb_scan_down<<<b->tot_stile, SCAN_THREADS, 0, s>>>(T);
     kb_scatter<<<b->tot_pblk, HASH_BLOCK, 0, s>>>(T);
-    kb_cell_fixup<<<b->tot_cblk, 256, 0, s>>>(T);
+    kb_cell_fixup<<<b->tot_cblk + (b->tot_itile + 255) / 256, 256, 0, s>>>(T);
     cudaError_t e = launch_gather_predict_batch(T, b->prec, b->tot_pblk, s);
     if (e == cudaSuccess) e = launch_interact_batch(T, b->lpp, b->cspm, b->cond, b->prec, b->num_sms, s);
     if (e != cudaSuccess) return fail(MFREE_ERR_CUDA, std::string("batched step launch: ") + cudaGetErrorString(e));
@@ -240,6 +253,7 @@ int mfree_batch_destroy(mfree_batch *b) {
             mfree_destroy(sl.c);
         }
     if (b->d_table) cudaFree(b->d_table);
+    if (b->d_tiles) cudaFree(b->d_tiles);
     for (auto e : b->timer)
         if (e) cudaEventDestroy(e);
     if (b->own_stream) cudaStreamDestroy(b->stream);

@@ -96,6 +96,8 @@ struct mfree_ctx {
     int graph_record_every = -1;
     // one-scene table of the batched kernels (ensure_table)
     unsigned char *d_table = nullptr;
+    int2 *d_tiles = nullptr;  // the pair kernel's list of non-empty tiles (grid-sized scratch)
+    int ntiles = 0;           // tiles of the grid at the table's depth
     mfree::BatchTable T{};
     unsigned long long table_version = ~0ull;
     int table_record_every = -1;
@@ -131,7 +133,7 @@ int clone_ctx(const mfree_ctx *c, cudaStream_t s, std::unique_ptr<mfree_ctx> &ou
 // waits for and frees the context's output job (mfree_output.cu)
 int finish_output(mfree_ctx *c, bool release);
 size_t scene_bytes(int n, long long num_cell);
-inline size_t single_table_bytes() { return 2 * sizeof(mfree::StepArgs) + 9 * sizeof(int); }
+inline size_t single_table_bytes() { return 2 * sizeof(mfree::StepArgs) + 10 * sizeof(int); }
 // device memory the context holds, in bytes
 size_t device_bytes(const mfree_ctx *c);
 

@@ -181,6 +181,8 @@ int ensure_scratch(mfree_ctx *c) {
     if ((st = dalloc(c, &c->scr.count, c->num_cell + 1, L))) return st;
     if ((st = dalloc(c, &c->scr.first, c->num_cell + 2 + SCAN_TILE, L))) return st;
     if ((st = dalloc(c, &c->scr.tile_sum, scan_tiles(c) + 1, L))) return st;
+    // the pair kernel's tile list: a tile of any depth holds a cell at least
+    if ((st = dalloc(c, &c->d_tiles, c->num_cell + 1, L))) return st;
     CUDA_TRY(cudaMemsetAsync(c->scr.count, 0, sizeof(int) * (c->num_cell + 1), c->stream));
     c->scratch_cells = size_t(c->num_cell);
     invalidate_graphs(c);
@@ -276,8 +278,8 @@ int ensure_table(mfree_ctx *c, int record_every) {
     }
     c->cur = keep;
     const Params &P = args[0].p;
-    const int ntiles = ((P.gnx + 3) / 4) * ((P.gny + 3) / 4) * ((P.gnz + P.tile_z - 1) / P.tile_z);
-    const int pre[9] = {0, hash_blocks(c), 0, scan_tiles(c), 0, int((c->num_cell + 255) / 256), 0, ntiles, 0};
+    const int ntiles = num_tiles(P);
+    const int pre[10] = {0, hash_blocks(c), 0, scan_tiles(c), 0, int((c->num_cell + 255) / 256), 0, ntiles, 0, 0};
     StepArgs *da = (StepArgs *)c->d_table;
     int *di = (int *)(da + 2);
     // pageable sources: the call returns once the bytes are staged
@@ -289,7 +291,10 @@ int ensure_table(mfree_ctx *c, int record_every) {
     c->T.cblk = di + 4;
     c->T.itile = di + 6;
     c->T.tile_next = di + 8;
+    c->T.tile_count = di + 9;
+    c->T.tile_list = c->d_tiles;
     c->T.nscenes = 1;
+    c->ntiles = ntiles;
     c->table_version = c->version;
     c->table_record_every = record_every;
     return MFREE_OK;
@@ -326,7 +331,7 @@ int enqueue_step(mfree_ctx *c, int record_mode, int record_every, bool timed = f
     run(3, [&] { kb_scan_top<<<1, 1024, 0, s>>>(T); });
     run(4, [&] { kb_scan_down<<<tiles, SCAN_THREADS, 0, s>>>(T); });
     run(5, [&] { kb_scatter<<<hb, HASH_BLOCK, 0, s>>>(T); });
-    run(6, [&] { kb_cell_fixup<<<int((c->num_cell + 255) / 256), 256, 0, s>>>(T); });
+    run(6, [&] { kb_cell_fixup<<<int((c->num_cell + 255) / 256) + (c->ntiles + 255) / 256, 256, 0, s>>>(T); });
     run(7, [&] { le = launch_gather_predict_batch(T, P.precision != 0, nb, s); });
     if (le == cudaSuccess)
         run(8, [&] { le = launch_interact_batch(T, lpp, P.cspm != 0, P.conduction, P.precision != 0, c->num_sms, s); });
@@ -446,6 +451,7 @@ size_t scene_bytes(int n, long long num_cell) {
     t += 3 * b(n, sizeof(int)) + b(hb + 1, sizeof(int)) + b(n, sizeof(int)) + 2 * b(n, sizeof(float4));
     t += b(fb * 3 * MAX_TOOLS, sizeof(float)) + b(1, sizeof(DevClock)) + b(3 * MAX_TOOLS, sizeof(float));
     t += b(num_cell + 1, sizeof(int)) + b(num_cell + 2 + SCAN_TILE, sizeof(int)) + b(tiles + 1, sizeof(int));
+    t += b(num_cell + 1, sizeof(int2));
     t += single_table_bytes();
     return t;
 }

@@ -296,7 +296,6 @@ __device__ void epilogue(const StepArgs &a, int i, const float *res) {
 // one bulk copy per column and array (cp.async.bulk, completion counted on an
 // mbarrier) stages into six shared-memory arrays.  A tile whose halo exceeds
 // the staging capacity reads the same records from global memory instead.
-constexpr int TX = 4, TY = 4;         // the depth (cells along z) is Params::tile_z
 constexpr int HX = TX + 4, HY = TY + 4;
 constexpr int CSROW = TILE_Z_MAX + 5;  // cell starts kept per halo column
 constexpr int NHC = HX * HY;           // halo columns
@@ -325,9 +324,12 @@ template <int LPP, int TILE_WARPS> struct TileSmem {
     int tstart[NTC];
     int tpref[NTC + 1];
     unsigned long long bar;
-    int tile, total, staged, parity, scene;
+    int tile, total, staged, parity, scene;  // scene < 0: no tile left
     int next_args;     // scene whose arguments the second args buffer holds (-1: none)
     int ntile, nscene; // the prologue threads' candidate tile
+    int2 pre_entry;    // tile-list entry fetched ahead for the next prologue
+    int pre_ok;        // pre_entry is being fetched (cp.async)
+    int list_n;        // entries of the tile list
 };
 __host__ __device__ constexpr size_t round128(size_t b) { return (b + 127) / 128 * 128; }
 // shared memory: the tables, the scene's arguments, the staged records
@@ -583,45 +585,52 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
 constexpr int PRO_FIRST = TCAP;
 __device__ __forceinline__ void pro_sync(int nthreads) { asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory"); }
 
-struct TileGeo {
-    int X0, Y0, Z0, zl, nzr;
-};
-__device__ __forceinline__ TileGeo tile_geo(const Params &P, int t) {
-    const int TZ = P.tile_z;
-    const int nty = (P.gny + TY - 1) / TY, ntz = (P.gnz + TZ - 1) / TZ;
-    const int tz = t % ntz, txy = t / ntz, ty = txy % nty, tx = txy / nty;
-    TileGeo g;
-    g.X0 = tx * TX;
-    g.Y0 = ty * TY;
-    g.Z0 = tz * TZ;
-    g.zl = max(g.Z0 - 2, 0);
-    g.nzr = min(g.Z0 + TZ + 1, P.gnz - 1) - g.zl + 2;  // cell starts per halo column (inclusive end)
-    return g;
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\ncp.async.commit_group;" ::"r"(smem_u32(dst)), "l"(src)
+                 : "memory");
 }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Run by the prologue threads: pulls tiles from the queue until a non-empty
-// one (or none is left), copies its scene's arguments into the second args
-// buffer when the scene is not the current tile's (busy_scene), builds its
-// target ranges, halo cell starts and halo offsets, and issues its staging
-// copies.  The prepared tile is left in sm.tile / sm.scene (tile = total:
-// none left).  The caller guarantees that nothing reads the staged records or
+// Run by the prologue threads: takes the next entry of the tile list (the
+// non-empty tiles of every scene), copies its scene's arguments into the
+// second args buffer when the scene is not the current tile's (busy_scene),
+// builds its halo cell starts, its target ranges (read from the halo table:
+// the target columns are halo columns) and halo offsets, and issues its
+// staging copies.  The prepared tile is left in sm.tile / sm.scene (scene < 0:
+// none left).  Each call claims the list entry of the next call at its start
+// and, once it has issued its copies, starts fetching that entry into shared
+// memory, so neither the claim's round trip nor the entry's load waits in the
+// next call.  The caller guarantees that nothing reads the staged records or
 // the tile tables any more.  Kept out of line: inlined into the kernel's loop
 // it made the pair rounds about 7% slower (measured on the 1M-particle step).
 template <int LPP, int W, int CAP>
 __device__ __noinline__ void prepare_tile(const BatchTable &T, TileSmem<LPP, W> &sm, StepArgs *sa, float4 *sarr,
-                                          int total, int busy_scene) {
+                                          int busy_scene) {
     constexpr int PT = W * 32 - PRO_FIRST;
     const int ptid = threadIdx.x - PRO_FIRST, pl = ptid & 31, pw = ptid >> 5;
+    int pend = -1;  // (thread 0 of the prologue) list index claimed by this call
     for (;;) {
         if (ptid == 0) {
-            const int t = atomicAdd(T.tile_next, 1);
-            sm.ntile = t;
-            sm.nscene = t < total ? find_scene(T.itile, T.nscenes, t) : -1;
+            const int n = sm.list_n;
+            int2 e = make_int2(0, -1);
+            if (pend >= 0) {  // after an empty entry (none are listed; kept for safety)
+                if (pend < n) e = T.tile_list[pend];
+            } else if (sm.pre_ok) {
+                cp_async_wait_all();
+                e = sm.pre_entry;
+            } else {
+                const int k = atomicAdd(T.tile_next, 1);
+                if (k < n) e = T.tile_list[k];
+            }
+            sm.pre_ok = 0;
+            pend = e.y >= 0 ? atomicAdd(T.tile_next, 1) : n;  // not waited for until the end
+            sm.ntile = e.x;
+            sm.nscene = e.y;
         }
         pro_sync(PT);
         const int t = sm.ntile, s = sm.nscene;
-        if (t >= total) {
-            if (ptid == 0) sm.tile = total;
+        if (s < 0) {
+            if (ptid == 0) sm.scene = -1;
             return;
         }
         // another scene's arguments go to the second buffer (the current
@@ -638,26 +647,8 @@ __device__ __noinline__ void prepare_tile(const BatchTable &T, TileSmem<LPP, W> 
         const StepArgs &a = sa[buf];
         const Params &P = a.p;
         const int nx = P.gnx, ny = P.gny, nz = P.gnz;
-        const TileGeo G = tile_geo(P, t - T.itile[s]);
+        const TileGeo G = tile_geo(P, t);
         const int *__restrict__ first = a.s.first;
-        if (pw == 0) {  // target column ranges: an empty tile ends here
-            const int c = pl;
-            int s0 = 0, len = 0;
-            if (c < NTC) {
-                const int cx = G.X0 + c / TY, cy = G.Y0 + c % TY;
-                if (cx < nx && cy < ny && G.Z0 < nz) {
-                    const int cb = (cx * ny + cy) * nz;
-                    s0 = first[cb + G.Z0];
-                    len = first[cb + min(G.Z0 + P.tile_z - 1, nz - 1) + 1] - s0;
-                }
-                sm.tstart[c] = s0;
-            }
-            const int ti = group_scan<32>(len, c);
-            if (c < NTC) sm.tpref[c] = ti - len;
-            if (c == 31) sm.tpref[NTC] = ti;
-        }
-        pro_sync(PT);
-        if (sm.tpref[NTC] == 0) continue;
         {  // halo cell starts, each thread's loads in flight together
             constexpr int NCS = (NHC * CSROW + PT - 1) / PT;
             int csv[NCS];
@@ -677,31 +668,52 @@ __device__ __noinline__ void prepare_tile(const BatchTable &T, TileSmem<LPP, W> 
             }
         }
         pro_sync(PT);
-        if (pw == 0) {  // prefix sum of the 64 halo columns; staging decision
-            int len2[2];
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int c = pl + 32 * h;
-                const int cx = G.X0 - 2 + c / HY, cy = G.Y0 - 2 + c % HY;
-                const bool in = cx >= 0 && cx < nx && cy >= 0 && cy < ny;
-                len2[h] = in ? sm.cellstart[c][G.nzr - 1] - sm.cellstart[c][0] : 0;
-                sm.hstart[c] = sm.cellstart[c][0];
-                sm.hlen[c] = len2[h];
+        if (pw == 0) {
+            // target column ranges (cells Z0 .. Z0 + depth - 1 of the 16
+            // target columns), then, for a non-empty tile, the prefix sum of
+            // the 64 halo columns and the staging decision
+            int len = 0;
+            if (pl < NTC) {
+                const int cx = G.X0 + pl / TY, cy = G.Y0 + pl % TY;
+                int s0 = 0;
+                if (cx < nx && cy < ny && G.Z0 < nz) {
+                    const int lc = (pl / TY + 2) * HY + (pl % TY + 2);
+                    s0 = sm.cellstart[lc][G.Z0 - G.zl];
+                    len = sm.cellstart[lc][min(G.Z0 + P.tile_z - 1, nz - 1) + 1 - G.zl] - s0;
+                }
+                sm.tstart[pl] = s0;
             }
-            const int i0 = group_scan<32>(len2[0], pl);
-            const int t0 = __shfl_sync(0xffffffffu, i0, 31);
-            const int i1 = group_scan<32>(len2[1], pl);
-            sm.hoff[pl] = i0 - len2[0];
-            sm.hoff[pl + 32] = t0 + i1 - len2[1];
-            const int tot = t0 + __shfl_sync(0xffffffffu, i1, 31);
-            if (pl == 0) {
-                sm.total = tot;
-                sm.staged = tot <= CAP ? 1 : 0;
-                if (sm.staged && tot > 0)
-                    mbar_expect(&sm.bar, unsigned(tot) * unsigned(REC_N * sizeof(float4)) + unsigned(P.stage_extra));
+            const int ti = group_scan<32>(len, pl);
+            if (pl < NTC) sm.tpref[pl] = ti - len;
+            if (pl == 31) sm.tpref[NTC] = ti;
+            if (__shfl_sync(0xffffffffu, ti, 31) > 0) {
+                int len2[2];
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int c = pl + 32 * h;
+                    const int cx = G.X0 - 2 + c / HY, cy = G.Y0 - 2 + c % HY;
+                    const bool in = cx >= 0 && cx < nx && cy >= 0 && cy < ny;
+                    len2[h] = in ? sm.cellstart[c][G.nzr - 1] - sm.cellstart[c][0] : 0;
+                    sm.hstart[c] = sm.cellstart[c][0];
+                    sm.hlen[c] = len2[h];
+                }
+                const int i0 = group_scan<32>(len2[0], pl);
+                const int t0 = __shfl_sync(0xffffffffu, i0, 31);
+                const int i1 = group_scan<32>(len2[1], pl);
+                sm.hoff[pl] = i0 - len2[0];
+                sm.hoff[pl + 32] = t0 + i1 - len2[1];
+                const int tot = t0 + __shfl_sync(0xffffffffu, i1, 31);
+                if (pl == 0) {
+                    sm.total = tot;
+                    sm.staged = tot <= CAP ? 1 : 0;
+                    if (sm.staged && tot > 0)
+                        mbar_expect(&sm.bar,
+                                    unsigned(tot) * unsigned(REC_N * sizeof(float4)) + unsigned(P.stage_extra));
+                }
             }
         }
         pro_sync(PT);
+        if (sm.tpref[NTC] == 0) continue;  // an empty tile: take the next
         if (sm.staged && sm.total > 0) {
             const float4 *gbase = a.r.f[0];  // the record arrays are one allocation: f[k] = f[0] + k * n_init
             for (int q = ptid; q < REC_N * NHC; q += PT) {
@@ -715,6 +727,9 @@ __device__ __noinline__ void prepare_tile(const BatchTable &T, TileSmem<LPP, W> 
         if (ptid == 0) {
             sm.tile = t;
             sm.scene = s;
+            if (pend < sm.list_n) cp_async8(&sm.pre_entry, T.tile_list + pend);
+            else sm.pre_entry = make_int2(0, -1);
+            sm.pre_ok = 1;
         }
         return;
     }
@@ -725,6 +740,7 @@ template <class SM> __device__ __forceinline__ void init_tile_smem(SM &sm) {
         mbar_init(&sm.bar, 1);
         sm.parity = 0;
         sm.next_args = -1;
+        sm.pre_ok = 0;
     }
     fence_proxy_async();
     __syncthreads();
@@ -749,16 +765,16 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
     float4 *sarr = reinterpret_cast<float4 *>(dyn + rec_offset<LPP, W>());
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane / LPP, sl = lane - g * LPP;
+    if (threadIdx.x == 0) sm.list_n = *T.tile_count;
     init_tile_smem(sm);
-    const int total = T.itile[T.nscenes];
     int cur = -1;
-    if (threadIdx.x >= PRO_FIRST) prepare_tile<LPP, W, CAP>(T, sm, sa, sarr, total, cur);
+    if (threadIdx.x >= PRO_FIRST) prepare_tile<LPP, W, CAP>(T, sm, sa, sarr, cur);
     const StepArgs &a = sa[0];
     for (;;) {
         __syncthreads();  // the prepared tile's descriptor and tables are visible
-        const int tile = sm.tile;
-        if (tile >= total) break;
         const int s = sm.scene;
+        if (s < 0) break;
+        const int tile = sm.tile;
         if (s != cur) {  // a new scene: its arguments wait in the second buffer
             const int4 *src = reinterpret_cast<const int4 *>(sa + 1);
             int4 *d = reinterpret_cast<int4 *>(sa);
@@ -766,7 +782,7 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
             __syncthreads();
             cur = s;
         }
-        const TileGeo geo = tile_geo(a.p, tile - T.itile[s]);
+        const TileGeo geo = tile_geo(a.p, tile);
         const int X0 = geo.X0, Y0 = geo.Y0, zl = geo.zl;
         const float4 *gbase = a.r.f[0];
         const int gstride = a.p.n_init;
@@ -790,6 +806,7 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
                 const long long t2 = clock64();
                 while (!mbar_try(&sm.bar, par) && clock64() - t2 <= WAIT_CYCLES) {
                 }
+                cp_async_wait_all();  // the prologue's fetch of the next list entry
                 return;
             }
             if (threadIdx.x == 0) sm.parity ^= 1;
@@ -854,7 +871,7 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
             if (threadIdx.x < PRO_FIRST) {
                 if (threadIdx.x < tn) epilogue<PREC, COND>(a, sm.tgt[threadIdx.x], sm.res[threadIdx.x]);
             } else if (last) {
-                prepare_tile<LPP, W, CAP>(T, sm, sa, sarr, total, s);
+                prepare_tile<LPP, W, CAP>(T, sm, sa, sarr, s);
             }
             if (!last) __syncthreads();
         }

@@ -83,8 +83,33 @@ struct BatchTable {
     const int *cblk;       // cell blocks of 256 threads (cell fix-up)
     const int *itile;      // pair-kernel tiles
     int nscenes;
-    int *tile_next;        // work queue of the pair kernel (reset by kb_clock)
+    int *tile_next;        // work queue of the pair kernel: next entry of tile_list (reset by kb_clock)
+    int *tile_count;       // entries of tile_list (reset by kb_clock)
+    int2 *tile_list;       // non-empty pair-kernel tiles of every scene: (tile of the scene, scene)
 };
+
+// Pair-kernel tile = TX x TY x tile_z cells of a scene's cell grid, numbered
+// z fastest, then y, then x
+constexpr int TX = 4, TY = 4;
+struct TileGeo {
+    int X0, Y0, Z0, zl, nzr;
+};
+__host__ __device__ __forceinline__ TileGeo tile_geo(const Params &P, int t) {
+    const int TZ = P.tile_z;
+    const int nty = (P.gny + TY - 1) / TY, ntz = (P.gnz + TZ - 1) / TZ;
+    const int tz = t % ntz, txy = t / ntz, ty = txy % nty, tx = txy / nty;
+    TileGeo g;
+    g.X0 = tx * TX;
+    g.Y0 = ty * TY;
+    g.Z0 = tz * TZ;
+    g.zl = g.Z0 - 2 > 0 ? g.Z0 - 2 : 0;
+    const int zh = g.Z0 + TZ + 1 < P.gnz - 1 ? g.Z0 + TZ + 1 : P.gnz - 1;
+    g.nzr = zh - g.zl + 2;  // cell starts per halo column of the tile (inclusive end)
+    return g;
+}
+__host__ __device__ __forceinline__ int num_tiles(const Params &P) {
+    return ((P.gnx + TX - 1) / TX) * ((P.gny + TY - 1) / TY) * ((P.gnz + P.tile_z - 1) / P.tile_z);
+}
 
 // scene of block x: the last s with prefix[s] <= x (prefix has nscenes + 1 entries)
 __device__ __forceinline__ int find_scene(const int *__restrict__ prefix, int nscenes, int x) {

@@ -67,7 +67,10 @@ __device__ __forceinline__ void clock_body(const StepArgs &a, int record_mode) {
 // one thread per scene; thread 0 also resets the batch's pair-kernel queue
 __global__ void kb_clock(BatchTable T, int record_mode) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s == 0) *T.tile_next = 0;
+    if (s == 0) {
+        *T.tile_next = 0;
+        *T.tile_count = 0;
+    }
     if (s < T.nscenes) clock_body(T.args[2 * s], record_mode);
 }
 
@@ -285,7 +288,50 @@ __device__ __forceinline__ void cell_fixup_body(const StepArgs &a, int bid) {
     }
 }
 __global__ void __launch_bounds__(256) k_cell_fixup(StepArgs a) { cell_fixup_body(a, blockIdx.x); }
+
+// The pair kernel's list of non-empty tiles: one thread per tile of every
+// scene; a tile with a particle in one of its target cells is appended as
+// (tile of its scene, scene), one atomic per warp.  The order of the list
+// changes which block runs a tile, never a result.
+__device__ __forceinline__ void tile_list_body(const BatchTable &T, int g) {
+    const int total = T.itile[T.nscenes];
+    bool ne = false;
+    int s = 0, t = 0;
+    if (g < total) {
+        s = find_scene(T.itile, T.nscenes, g);
+        t = g - T.itile[s];
+        const StepArgs *a0 = T.args + 2 * s;
+        const StepArgs &a = a0[a0->clk->parity & 1];
+        const Params &P = a.p;
+        const int nx = P.gnx, ny = P.gny, nz = P.gnz;
+        const TileGeo G = tile_geo(P, t);
+        const int zend = min(G.Z0 + P.tile_z - 1, nz - 1) + 1;
+        const int *__restrict__ first = a.s.first;
+        for (int c = 0; c < TX * TY; c++) {
+            const int cx = G.X0 + c / TY, cy = G.Y0 + c % TY;
+            if (cx < nx && cy < ny && G.Z0 < nz) {
+                const int cb = (cx * ny + cy) * nz;
+                ne |= first[cb + zend] > first[cb + G.Z0];
+            }
+        }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, ne);
+    if (m == 0) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(T.tile_count, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (ne) T.tile_list[base + __popc(m & ((1u << lane) - 1u))] = make_int2(t, s);
+}
+
+// blocks past the cell blocks of every scene build the tile list (the cell
+// starts are final once the scatter has run)
 __global__ void __launch_bounds__(256) kb_cell_fixup(BatchTable T) {
+    const int nb = T.cblk[T.nscenes];
+    if (int(blockIdx.x) >= nb) {
+        tile_list_body(T, (int(blockIdx.x) - nb) * 256 + int(threadIdx.x));
+        return;
+    }
     run_batched(T, T.cblk, [](const StepArgs &a, int b) { cell_fixup_body(a, b); });
 }
 
