@@ -314,6 +314,7 @@ template <int LPP, int TILE_WARPS> struct TileSmem {
     static constexpr int G = 32 / LPP;
     float res[TCAP][NRES + 1];
     int tgt[TCAP];       // sorted index of each target of the pass
+    int tcell[TCAP];     // its cell: target column << 16 | z
     int q[TILE_WARPS][G][QCAP_T];
     int cbase[TILE_WARPS][G][25];
     int cpref[TILE_WARPS][G][26];
@@ -394,11 +395,11 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
     const float4 *__restrict__ rB = RF + REC_B * rstride;
     const float4 *__restrict__ rR = RF + REC_R * rstride;
     const float4 *__restrict__ rC = RF + REC_C * rstride;
-    // the target's cell; its own records come from the staged halo (its cell
-    // column is one of the halo's) or from global memory
-    const unsigned key = a.s.key_sorted[i];
-    const int nyz = ny * nz;
-    const int gi = int(key) / nyz, rem = int(key) - gi * nyz, gj = rem / nz, gk = rem - gj * nz;
+    // the target's cell (from the pass's target table); its own records come
+    // from the staged halo (its cell column is one of the halo's) or from
+    // global memory
+    const int tcell = sm.tcell[valid ? tt : 0];
+    const int gi = X0 + (tcell >> 16) / TY, gj = Y0 + (tcell >> 16) % TY, gk = tcell & 0xffff;
     IData I;
     {
         int si = i;
@@ -818,7 +819,14 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
                 const int tg = t0 + tt;
                 int c = 0;
                 while (c < NTC - 1 && sm.tpref[c + 1] <= tg) c++;
-                sm.tgt[tt] = sm.tstart[c] + (tg - sm.tpref[c]);
+                const int i = sm.tstart[c] + (tg - sm.tpref[c]);
+                sm.tgt[tt] = i;
+                // its cell: the z row of its column whose range holds i (the
+                // rows up to the tile's last target cell are in the table)
+                const int *cs = sm.cellstart[(c / TY + 2) * HY + (c % TY + 2)];
+                int k = geo.Z0 - zl;
+                while (cs[k + 1] <= i) k++;
+                sm.tcell[tt] = (c << 16) | (zl + k);
             }
             __syncthreads();
             // rounds of TILE_WARPS * G targets; a last round with few targets
