@@ -316,8 +316,9 @@ template <int LPP, int TILE_WARPS> struct TileSmem {
     int tgt[TCAP];       // sorted index of each target of the pass
     int tcell[TCAP];     // its cell: target column << 16 | z
     int q[TILE_WARPS][G][QCAP_T];
-    int cbase[TILE_WARPS][G][25];
-    int cpref[TILE_WARPS][G][26];
+    // per stencil column of a group's target: (end of its candidates in the
+    // flattened order, record index minus flattened index)
+    int2 cwalk[TILE_WARPS][G][25];
     int cellstart[NHC][CSROW];
     int hoff[NHC];       // staged offset of a halo column
     int hstart[NHC];     // global start of a halo column
@@ -417,9 +418,9 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
         I.h1 = 1.0f / I.h;
         I.fac = 0.31830988618379067f * I.h1 * I.h1 * I.h1;
     }
-    int *cb = sm.cbase[warp][g];
-    int *cp = sm.cpref[warp][g];
+    int2 *cw = sm.cwalk[warp][g];
     int *qq = sm.q[warp][g];
+    int total;  // candidates of the target
     // ---- the 25 stencil columns as ranges of the record arrays, with their prefix
     {
         const int klo = max(gk - 2, 0) - zl, khi = min(gk + 2, nz - 1) - zl + 1;
@@ -439,24 +440,22 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
                 }
             }
             const int inc = group_scan<LPP>(l, sl);
-            if (c < 25) {
-                cb[c] = b;
-                cp[c] = carry + inc - l;
-            }
+            if (c < 25) cw[c] = make_int2(carry + inc, b - (carry + inc - l));
             carry += __shfl_sync(0xffffffffu, inc, (g * LPP) + LPP - 1);
         }
-        if (sl == 0) cp[25] = carry;
+        total = carry;
     }
     __syncwarp();
     // ---- candidates: lane sl takes candidates sl, sl + LPP, ... of the
     // flattened stencil (consecutive lanes read consecutive records); the
     // column it is in is kept in registers and reloaded only on a crossing
-    const int total = cp[25];
     int maxtotal = total;
 #pragma unroll
     for (int o = 16; o >= LPP; o >>= 1) maxtotal = max(maxtotal, __shfl_xor_sync(0xffffffffu, maxtotal, o));
     auto scan = [&](auto &&fn) {
-        int col = 0, cend = cp[1], base = cb[0];  // base = cb[col] - cp[col]
+        int col = 0;
+        int2 w = cw[0];
+        int cend = w.x, base = w.y;
 #pragma unroll 2
         for (int k0 = 0; k0 < maxtotal; k0 += LPP) {
             const int k = k0 + sl;
@@ -464,8 +463,9 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
             if (act) {
                 while (k >= cend) {  // k < total keeps col <= 24
                     col++;
-                    cend = cp[col + 1];
-                    base = cb[col] - cp[col];
+                    w = cw[col];
+                    cend = w.x;
+                    base = w.y;
                 }
             }
             fn(base + k, act);
@@ -484,10 +484,10 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
             const float r2 = dist2_rn(dx, dy, dz);
             ins = !(r2 >= four_h2) && (r2 > 9.99999994e-9f);  // in_support()
             if (COND == MFREE_COND_PSE) {
-                const float4 Cj = rC[j];
+                const float2 tv = reinterpret_cast<const float2 *>(rC + j)[1];  // (T_j, V_j)
                 float e2;
                 asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e2) : "f"(pse_k * r2));
-                pse = fmaf((Cj.z - I.T) * Cj.w, e2, pse);
+                pse = fmaf((tv.x - I.T) * tv.y, e2, pse);
             }
         }
         const unsigned m = __ballot_sync(0xffffffffu, ins) & gmask;
