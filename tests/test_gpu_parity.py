@@ -94,6 +94,37 @@ def test_three_steps_against_fp64_oracle_full_size_1m():
     sim.close()
 
 
+def test_100_steps_against_fp64_oracle_full_size_1m_plain_and_precision():
+    """The 1,000,000-particle configuration (CSPM, artificial stress, PSE)
+    after 100 steps, run once in plain FP32 and once in the precision form
+    (compensated hi/lo positions and velocities), each against one FP64
+    oracle run: the per-field relative L2 error of both is printed, both stay
+    within the tolerances of the 8,000-particle 100-step test, and the
+    precision form's displacement error is no worse than plain FP32's."""
+    sc = scenes.million_scene()
+    plain = _sim(sc)
+    prec = _sim(sc, precision=1)
+    orc = oracle.Oracle(sc, prec=64)
+    for _ in range(100):
+        plain.step()
+        prec.step()
+        orc.step()
+    o = oracle_state(orc)
+    e_plain = compare(gpu_state(plain), o, sc)
+    e_prec = compare(gpu_state(prec, f64=True), o, sc)
+    for name, err in (("plain FP32", e_plain), ("precision form", e_prec)):
+        print(f"1M, 100-step relative L2 vs FP64 oracle, {name}: " +
+              ", ".join(f"{k} {v:.3e}" for k, v in err.items()))
+    tol = dict(POS=5e-3, VEL=5e-3, S=5e-3, EPS_PL=2e-2, T=2e-2, RHO=5e-3)
+    for err in (e_plain, e_prec):
+        assert err["blank_mismatch"] == 0
+        for k, v in tol.items():
+            assert err[k] < v, (k, err)
+    assert e_prec["POS"] <= 1.5 * e_plain["POS"]
+    plain.close()
+    prec.close()
+
+
 def test_one_step_against_fp32_oracle():
     """One step from the same input: the CUDA path against the oracle in the
     reference's FP32 semantics.  Differences come from summation order,
