@@ -75,6 +75,10 @@ typedef struct {
                                constant (tool_3d_gpu.cu:26,528), so 0 matches it.    */
     int tile_depth;         /* pair-loop tiling: cells per tile along z, 1..8; 0 picks
                                the tuned default (6).  Results do not depend on it.   */
+    int full_stencil;       /* 1: the pair loop visits every candidate of the 5x5x5
+                               cell stencil.  0 (default): without PSE conduction it
+                               skips the stencil cells that lie wholly beyond the
+                               target's support radius.  Results do not depend on it. */
 } mfree_options;
 
 /* ---- fields for mfree_get_field / mfree_set_field ------------------------
@@ -124,6 +128,9 @@ typedef struct {
                                    summed over steps                                    */
     int64_t staging_timeouts;   /* pair-kernel staging waits that ran out (each makes
                                    the next call return MFREE_ERR_TIMEOUT)              */
+    int64_t full_stencil_steps; /* steps whose pair loop fell back to the full 5x5x5
+                                   stencil because a particle moved too far in the
+                                   predictor (variants without PSE; see full_stencil) */
 } mfree_counters;
 
 typedef struct mfree_ctx mfree_ctx;
@@ -216,7 +223,10 @@ int mfree_sync(mfree_ctx *ctx);
 int mfree_get_counts(const mfree_ctx *ctx, int *n_active, int *n_init);
 /* count elements of one particle's entry of a field (4 for float4 ...) */
 int mfree_field_width(int field);
-/* copy a whole field (n_init entries) to / from host memory */
+/* copy a whole field (n_init entries) to / from host memory.  When out is
+ * page-locked (cudaMallocHost / cudaHostAlloc / cudaHostRegister) the state
+ * fields are written into it by the device in one pass; otherwise they are
+ * copied and converted on the host.  The values are the same either way. */
 int mfree_get_field(mfree_ctx *ctx, int field, void *out);
 int mfree_set_field(mfree_ctx *ctx, int field, const void *in);
 /* the same in double: MFREE_POS and MFREE_VEL return hi + lo of the

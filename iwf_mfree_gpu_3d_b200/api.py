@@ -77,12 +77,12 @@ class Joco(C.Structure):
 class Options(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("cspm", "conduction", "precision", "max_secant_iter",
                                        "lanes_per_particle", "diagnostics", "friction_tool_vel",
-                                       "tile_depth")]
+                                       "tile_depth", "full_stencil")]
 
 
 class Counters(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("steps", "secant_failures", "out_of_grid", "contact_search_cap",
-                                         "nan_blanked", "staging_timeouts")]
+                                         "nan_blanked", "staging_timeouts", "full_stencil_steps")]
 
 
 _lib = None
@@ -261,7 +261,7 @@ class Simulation:
 
     def set_options(self, **kw):
         o = Options(cspm=0, conduction=COND_BROOKSHAW, precision=0, max_secant_iter=100, lanes_per_particle=0,
-                    diagnostics=0, friction_tool_vel=0, tile_depth=0)
+                    diagnostics=0, friction_tool_vel=0, tile_depth=0, full_stencil=0)
         for k, v in kw.items():
             setattr(o, k, int(v))
         self._opt = o
@@ -384,13 +384,20 @@ class Simulation:
         _check(self.L.mfree_get_counters(self.h, C.byref(c)))
         return {k: getattr(c, k) for k, _ in Counters._fields_}
 
-    def get(self, name: str) -> np.ndarray:
+    def get(self, name: str, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """A whole field; ``out`` (C-contiguous, n_init x width entries of the
+        field's dtype) is filled instead of a new array -- page-locked memory
+        there lets the device write the field directly."""
         f = FIELD_ID[name]
         w = self.L.mfree_field_width(f)
         dt = np.int32 if name in INT_FIELDS else np.float32
-        out = np.zeros(self.n_init * w, dt)
+        if out is None:
+            out = np.zeros(self.n_init * w, dt)
+        elif out.dtype != dt or out.size != self.n_init * w or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"get({name!r}): out must be a C-contiguous {np.dtype(dt).name} array of "
+                             f"{self.n_init * w} entries")
         _check(self.L.mfree_get_field(self.h, f, out.ctypes.data_as(C.c_void_p)))
-        return out.reshape(self.n_init, w) if w > 1 else out
+        return out.reshape(self.n_init, w) if w > 1 else out.reshape(-1)
 
     def get64(self, name: str) -> np.ndarray:
         f = FIELD_ID[name]

@@ -48,12 +48,14 @@ struct DevClock {
     int record;       // record tool forces this step
     int staging_timeouts;  // pair-kernel staging waits that ran out (that block left its tiles undone)
     int parity;       // which of the two state copies holds this step's input (flips every step)
+    int prune_off;    // 1: a particle moved more than PRUNE_DISP cells in this step's predictor, so the
+                      // pair kernel visits the full stencil (reset by the clock kernel every step)
     long long step_index;
     float blank_min[3], blank_max[3];
     float grid_min[3];
     ToolClock tool[MAX_TOOLS];
     // device-detected conditions (mfree_counters)
-    unsigned long long secant_failures, out_of_grid, contact_cap, nan_blanked;
+    unsigned long long secant_failures, out_of_grid, contact_cap, nan_blanked, full_stencil_steps;
 };
 
 struct ToolDev {
@@ -101,7 +103,17 @@ struct Params {
     int record_every;
     int tile_z;  // cells per pair-kernel tile along z (1..TILE_Z_MAX)
     int stage_extra;  // bytes added to the staging byte count: nonzero only to make the waits run out (tests)
+    int full_stencil;  // 1: the pair kernel visits every stencil candidate (no geometric pruning)
 };
+
+// Geometric pruning of the pair kernel's stencil (variants without PSE): a
+// candidate lies in the cell its position at the hash gave it, and the
+// predictor moves it by at most PRUNE_DISP cells per axis (checked every step
+// by the predictor; a larger move switches the step to the full stencil).
+// PRUNE_MARGIN adds slack for the rounding of the hash and of the distance
+// arithmetic (both ~1e-7 relative, against ~4e-3 cells of slack).
+constexpr float PRUNE_DISP = 1.0f / 64.0f;
+constexpr float PRUNE_MARGIN = PRUNE_DISP + 1.0f / 256.0f;
 
 struct State {
     float4 *pos4, *vel4, *sa4, *sb4, *da4, *dv4, *dsa4, *dsb4, *fc4, *ft4, *bc4, *lo4, *lo4b;

@@ -105,6 +105,7 @@ Params make_params(const mfree_ctx *c) {
     P.precision = c->opt.precision;
     P.diagnostics = c->opt.diagnostics;
     P.friction_tool_vel = c->opt.friction_tool_vel;
+    P.full_stencil = c->opt.full_stencil ? 1 : 0;
     P.gnx = int(c->nx);
     P.gny = int(c->ny);
     P.gnz = int(c->nz);
@@ -938,6 +939,7 @@ int mfree_get_counters(mfree_ctx *c, mfree_counters *o) {
     o->contact_search_cap = int64_t(h.contact_cap);
     o->nan_blanked = int64_t(h.nan_blanked);
     o->staging_timeouts = int64_t(h.staging_timeouts);
+    o->full_stencil_steps = int64_t(h.full_stencil_steps);
     return MFREE_OK;
 }
 
@@ -959,9 +961,87 @@ inline void sym_to_9(const float s[6], float *o) {
     o[6] = s[4]; o[7] = s[5]; o[8] = s[2];
 }
 
+// One field of the state in the reference layout, written by the device
+// straight into page-locked host memory (dst is its device alias).  A block's
+// 256 entries are assembled in shared memory and stored as one contiguous run,
+// so the writes that cross the host link are whole lines.  Fields the kernel
+// does not know (returns false) go through the host path below.
+__host__ __device__ constexpr bool field_on_device(int f) {
+    return f == MFREE_POS || f == MFREE_VEL || f == MFREE_VEL_BC || f == MFREE_H || f == MFREE_RHO || f == MFREE_S ||
+           f == MFREE_S_T || f == MFREE_FC || f == MFREE_FT || f == MFREE_POS_T || f == MFREE_VEL_T ||
+           f == MFREE_FIXED || f == MFREE_EPS_PL_DOT || f == MFREE_BLANKED || f == MFREE_TOOL_PARTICLE ||
+           f == MFREE_EPS_PL || f == MFREE_T || f == MFREE_RHO_T || f == MFREE_T_T || f == MFREE_ID;
+}
+
+__global__ void __launch_bounds__(256) k_get_field(int f, int w, State S, int n, float *dst) {
+    __shared__ float buf[256 * 9];
+    const int i0 = blockIdx.x * 256, i = i0 + threadIdx.x;
+    if (i < n) {
+        float *o = buf + threadIdx.x * w;
+        auto xyz = [&](float4 v) { o[0] = v.x; o[1] = v.y; o[2] = v.z; if (w == 4) o[3] = 0.f; };
+        auto sym9 = [&](float4 a, float4 b) {  // (xx yy zz xy) (xz yz): GLM column-major 3x3
+            o[0] = a.x; o[1] = a.w; o[2] = b.x;
+            o[3] = a.w; o[4] = a.y; o[5] = b.y;
+            o[6] = b.x; o[7] = b.y; o[8] = a.z;
+        };
+        switch (f) {
+            case MFREE_POS: xyz(S.pos4[i]); break;
+            case MFREE_VEL: xyz(S.vel4[i]); break;
+            case MFREE_VEL_BC: xyz(S.bc4[i]); break;
+            case MFREE_H: o[0] = S.pos4[i].w; break;
+            case MFREE_RHO: o[0] = S.vel4[i].w; break;
+            case MFREE_S: sym9(S.sa4[i], S.sb4[i]); break;
+            case MFREE_S_T: sym9(S.dsa4[i], S.dsb4[i]); break;
+            case MFREE_FC: xyz(S.fc4[i]); break;
+            case MFREE_FT: xyz(S.ft4[i]); break;
+            case MFREE_POS_T: xyz(S.da4[i]); break;
+            case MFREE_VEL_T: xyz(S.dv4[i]); break;
+            case MFREE_FIXED: o[0] = S.dsb4[i].w; break;
+            case MFREE_EPS_PL_DOT: o[0] = S.dsb4[i].z; break;
+            case MFREE_BLANKED: o[0] = S.ft4[i].w; break;
+            case MFREE_TOOL_PARTICLE: o[0] = S.fc4[i].w; break;
+            case MFREE_EPS_PL: o[0] = S.sb4[i].w; break;
+            case MFREE_T: o[0] = S.sb4[i].z; break;
+            case MFREE_RHO_T: o[0] = S.da4[i].w; break;
+            case MFREE_T_T: o[0] = S.dv4[i].w; break;
+            case MFREE_ID: o[0] = S.bc4[i].w; break;  // the id's int bits
+            default: break;
+        }
+    }
+    __syncthreads();
+    const int cnt = min(256, n - i0) * w;
+    float *d = dst + size_t(i0) * w;
+    for (int k = threadIdx.x; k < cnt; k += 256) d[k] = buf[k];
+}
+
+// the device path of mfree_get_field: 1 when done, 0 when out is not
+// page-locked memory the device can write (the host path then runs)
+int get_field_pinned(mfree_ctx *c, int f, float *out, int *st) {
+    *st = MFREE_OK;
+    if (!field_on_device(f)) return 0;
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, out) != cudaSuccess) {
+        cudaGetLastError();  // not a pointer CUDA knows: clear the error
+        return 0;
+    }
+    if (at.type != cudaMemoryTypeHost || !at.devicePointer) return 0;
+    const int n = c->n_init, w = mfree_field_width(f);
+    if (n > 0) {
+        k_get_field<<<(n + 255) / 256, 256, 0, c->stream>>>(f, w, c->st[c->cur], n, (float *)at.devicePointer);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) *st = fail(MFREE_ERR_CUDA, std::string("mfree_get_field: ") + cudaGetErrorString(e));
+    }
+    return 1;
+}
+
 int get_field_impl(mfree_ctx *c, int f, float *fo, double *dout) {
     const int n = c->n_init;
     const State &S = c->st[c->cur];
+    if (fo && !dout) {
+        int st = MFREE_OK;
+        if (get_field_pinned(c, f, fo, &st)) return st;
+    }
     std::vector<float4> A, B, C;
     int st = 0;
     const int w = mfree_field_width(f);

@@ -326,6 +326,7 @@ template <int LPP, int TILE_WARPS> struct TileSmem {
     int tstart[NTC];
     int tpref[NTC + 1];
     unsigned long long bar;
+    float4 org;        // stencil pruning of the current tile's scene: grid origin, 1 = on (no PSE only)
     int tile, total, staged, parity, scene;  // scene < 0: no tile left
     int next_args;     // scene whose arguments the second args buffer holds (-1: none)
     int ntile, nscene; // the prologue threads' candidate tile
@@ -421,9 +422,28 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
     int2 *cw = sm.cwalk[warp][g];
     int *qq = sm.q[warp][g];
     int total;  // candidates of the target
-    // ---- the 25 stencil columns as ranges of the record arrays, with their prefix
+    // ---- the 25 stencil columns as ranges of the record arrays, with their
+    // prefix.  Without PSE (which sums every candidate of the 5x5x5 cells) the
+    // cells that lie wholly beyond the target's support radius are left out
+    // (org.w != 0; org.xyz = the grid origin of this step's hash): in cell
+    // units, a column's x-y box and a cell's z extent, each widened by
+    // PRUNE_MARGIN, against the sphere of radius 2h around the target.  Only
+    // out-of-support candidates go, in the same order, so the in-support
+    // queue and every sum over it are unchanged.  Cell 0 of an axis also holds
+    // positions up to one cell below the origin (the hash truncates toward 0).
+    constexpr bool PRUNE = COND != MFREE_COND_PSE;
+    const float4 org = PRUNE ? sm.org : make_float4(0.f, 0.f, 0.f, 0.f);
+    float ux = 0.f, uy = 0.f, uz = 0.f, rc2 = 0.f;
+    if (PRUNE && org.w != 0.f) {
+        const float ic = 1.0f / P.gdx;
+        ux = (I.x - org.x) * ic;
+        uy = (I.y - org.y) * ic;
+        uz = (I.z - org.z) * ic;
+        const float rc = 2.0f * I.h * ic;
+        rc2 = rc * rc;
+    }
     {
-        const int klo = max(gk - 2, 0) - zl, khi = min(gk + 2, nz - 1) - zl + 1;
+        const int klo = max(gk - 2, 0), khi = min(gk + 2, nz - 1);
         constexpr int NSET = (25 + LPP - 1) / LPP;
         int carry = 0;
 #pragma unroll
@@ -433,10 +453,29 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
             if (valid && c < 25) {
                 const int cx = gi + c / 5 - 2, cy = gj + c % 5 - 2;
                 if (cx >= 0 && cx < nx && cy >= 0 && cy < ny) {
-                    const int lc = (cx - X0 + 2) * HY + (cy - Y0 + 2);
-                    const int s0 = sm.cellstart[lc][klo];
-                    l = sm.cellstart[lc][khi] - s0;
-                    b = STAGED ? sm.hoff[lc] + (s0 - sm.hstart[lc]) : s0;
+                    int k0 = klo, k1 = khi;
+                    if (PRUNE && org.w != 0.f) {
+                        const float lox = (cx == 0 ? -1.f : float(cx)) - PRUNE_MARGIN;
+                        const float loy = (cy == 0 ? -1.f : float(cy)) - PRUNE_MARGIN;
+                        const float ex = fmaxf(0.f, fmaxf(lox - ux, ux - (float(cx + 1) + PRUNE_MARGIN)));
+                        const float ey = fmaxf(0.f, fmaxf(loy - uy, uy - (float(cy + 1) + PRUNE_MARGIN)));
+                        const float d2 = ex * ex + ey * ey;
+                        if (d2 < rc2) {
+                            const float zr = sqrtf(rc2 - d2) + PRUNE_MARGIN;
+                            int z1 = int(floorf(uz + zr));
+                            if (z1 < 0 && uz + zr > -1.f) z1 = 0;
+                            k0 = max(k0, int(floorf(uz - zr)));
+                            k1 = min(k1, z1);
+                        } else {
+                            k1 = k0 - 1;
+                        }
+                    }
+                    if (k1 >= k0) {
+                        const int lc = (cx - X0 + 2) * HY + (cy - Y0 + 2);
+                        const int s0 = sm.cellstart[lc][k0 - zl];
+                        l = sm.cellstart[lc][k1 + 1 - zl] - s0;
+                        b = STAGED ? sm.hoff[lc] + (s0 - sm.hstart[lc]) : s0;
+                    }
                 }
             }
             const int inc = group_scan<LPP>(l, sl);
@@ -789,6 +828,14 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
         const int gstride = a.p.n_init;
         const int ntg = sm.tpref[NTC];
         const bool staged = sm.staged != 0;
+        if (COND != MFREE_COND_PSE && threadIdx.x == 0) {  // read by the targets after the next barrier
+            float4 org = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (!a.p.full_stencil && !a.clk->prune_off) {
+                const float *gm = a.p.grid_moving ? a.clk->grid_min : a.p.grid_min0;
+                org = make_float4(gm[0], gm[1], gm[2], 1.f);
+            }
+            sm.org = org;
+        }
         if (staged && sm.total > 0) {
             const unsigned par = unsigned(sm.parity);
             const long long t_wait = clock64();

@@ -43,6 +43,7 @@ __device__ __forceinline__ void clock_body(const StepArgs &a, int record_mode) {
         c->parity ^= 1;      // the last step's output is this step's input
     }
     c->pending = 1;
+    c->prune_off = 0;
     const float t = c->t;
     c->record = record_mode == 1 ? 1
                 : record_mode == 2 ? (P.record_every > 0 && (c->step_index % P.record_every) == 0)
@@ -364,6 +365,11 @@ template <bool PREC> __device__ __forceinline__ void gather_predict_body(const S
     if (i >= N) return;  // blanked: frozen
     const float h2 = 0.5f * P.dt;
     HalfStep hs = half_step<PREC>(h2, pos, vel, sa, sb, da, dv, dsa, dsb, lo, lob);
+    {   // the pair kernel's stencil pruning assumes a move of at most PRUNE_DISP cells
+        const float lim = PRUNE_DISP * P.gdx;
+        if (!(fabsf(hs.x - pos.x) <= lim && fabsf(hs.y - pos.y) <= lim && fabsf(hs.z - pos.z) <= lim))
+            if (atomicExch(&a.clk->prune_off, 1) == 0) atomicAdd(&a.clk->full_stencil_steps, 1ull);
+    }
     const bool tool = fc.w == 1.f;
     float prs = 0.f;
     float Rr[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};

@@ -110,3 +110,22 @@ def test_tool_and_blanking_vtk_and_force_log(tmp_path):
     last = [float(v) for v in log[2].split()]
     np.testing.assert_allclose(last, f_last.reshape(-1), rtol=1e-8)
     sim.close()
+
+
+def test_fields_into_page_locked_memory_equal_the_host_path():
+    """mfree_get_field into page-locked memory (the device writes the field in
+    the reference layout) gives the same bits as into pageable memory (copied
+    and converted on the host), for every state field, in both forms."""
+    import torch
+
+    for precision in (0, 1):
+        sim = api.Simulation.from_scene(scenes.small_scene(), precision=precision)
+        sim.advance(7, use_graph=True)
+        for name in ("POS", "VEL", "VEL_BC", "H", "RHO", "S", "S_T", "FC", "FT", "POS_T", "VEL_T", "FIXED",
+                     "EPS_PL_DOT", "BLANKED", "TOOL_PARTICLE", "EPS_PL", "T", "RHO_T", "T_T", "ID", "IDX", "HASH"):
+            ref = sim.get(name)
+            tdt = torch.int32 if ref.dtype == np.int32 else torch.float32
+            pinned = torch.full((ref.size,), -7, dtype=tdt, pin_memory=True).numpy()
+            got = sim.get(name, out=pinned)
+            np.testing.assert_array_equal(got.view(np.uint32), ref.view(np.uint32), err_msg=name)
+        sim.close()
