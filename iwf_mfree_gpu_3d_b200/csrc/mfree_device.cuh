@@ -48,8 +48,8 @@ struct DevClock {
     int record;       // record tool forces this step
     int staging_timeouts;  // pair-kernel staging waits that ran out (that block left its tiles undone)
     int parity;       // which of the two state copies holds this step's input (flips every step)
-    int prune_off;    // 1: a particle moved more than PRUNE_DISP cells in this step's predictor, so the
-                      // pair kernel visits the full stencil (reset by the clock kernel every step)
+    unsigned max_disp;  // float bits: the largest move of a particle in this step's predictor, in cells
+                        // (the pair kernel's stencil-pruning margin; reset by the clock kernel every step)
     long long step_index;
     float blank_min[3], blank_max[3];
     float grid_min[3];
@@ -107,13 +107,14 @@ struct Params {
 };
 
 // Geometric pruning of the pair kernel's stencil (variants without PSE): a
-// candidate lies in the cell its position at the hash gave it, and the
-// predictor moves it by at most PRUNE_DISP cells per axis (checked every step
-// by the predictor; a larger move switches the step to the full stencil).
-// PRUNE_MARGIN adds slack for the rounding of the hash and of the distance
-// arithmetic (both ~1e-7 relative, against ~4e-3 cells of slack).
-constexpr float PRUNE_DISP = 1.0f / 64.0f;
-constexpr float PRUNE_MARGIN = PRUNE_DISP + 1.0f / 256.0f;
+// candidate lies in the cell its position at the hash gave it, moved by the
+// predictor.  The predictor records the step's largest move per axis (in
+// cells); the pair kernel widens every cell by that plus PRUNE_SLACK, which
+// covers the rounding of the hash and of the distance arithmetic (~1e-7
+// relative, against ~4e-3 cells).  A move beyond PRUNE_DISP_MAX cells (or a
+// NaN) switches the step to the full stencil.
+constexpr float PRUNE_DISP_MAX = 0.25f;
+constexpr float PRUNE_SLACK = 1.0f / 256.0f;
 
 struct State {
     float4 *pos4, *vel4, *sa4, *sb4, *da4, *dv4, *dsa4, *dsb4, *fc4, *ft4, *bc4, *lo4, *lo4b;

@@ -425,9 +425,10 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
     // ---- the 25 stencil columns as ranges of the record arrays, with their
     // prefix.  Without PSE (which sums every candidate of the 5x5x5 cells) the
     // cells that lie wholly beyond the target's support radius are left out
-    // (org.w != 0; org.xyz = the grid origin of this step's hash): in cell
-    // units, a column's x-y box and a cell's z extent, each widened by
-    // PRUNE_MARGIN, against the sphere of radius 2h around the target.  Only
+    // (org.w = the margin in cells, 0 = off; org.xyz = the grid origin of this
+    // step's hash): in cell units, a column's x-y box and a cell's z extent,
+    // each widened by the margin, against the sphere of radius 2h around the
+    // target.  Only
     // out-of-support candidates go, in the same order, so the in-support
     // queue and every sum over it are unchanged.  Cell 0 of an axis also holds
     // positions up to one cell below the origin (the hash truncates toward 0).
@@ -455,13 +456,14 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
                 if (cx >= 0 && cx < nx && cy >= 0 && cy < ny) {
                     int k0 = klo, k1 = khi;
                     if (PRUNE && org.w != 0.f) {
-                        const float lox = (cx == 0 ? -1.f : float(cx)) - PRUNE_MARGIN;
-                        const float loy = (cy == 0 ? -1.f : float(cy)) - PRUNE_MARGIN;
-                        const float ex = fmaxf(0.f, fmaxf(lox - ux, ux - (float(cx + 1) + PRUNE_MARGIN)));
-                        const float ey = fmaxf(0.f, fmaxf(loy - uy, uy - (float(cy + 1) + PRUNE_MARGIN)));
+                        const float mg = org.w;
+                        const float lox = (cx == 0 ? -1.f : float(cx)) - mg;
+                        const float loy = (cy == 0 ? -1.f : float(cy)) - mg;
+                        const float ex = fmaxf(0.f, fmaxf(lox - ux, ux - (float(cx + 1) + mg)));
+                        const float ey = fmaxf(0.f, fmaxf(loy - uy, uy - (float(cy + 1) + mg)));
                         const float d2 = ex * ex + ey * ey;
                         if (d2 < rc2) {
-                            const float zr = sqrtf(rc2 - d2) + PRUNE_MARGIN;
+                            const float zr = sqrtf(rc2 - d2) + mg;
                             int z1 = int(floorf(uz + zr));
                             if (z1 < 0 && uz + zr > -1.f) z1 = 0;
                             k0 = max(k0, int(floorf(uz - zr)));
@@ -830,9 +832,10 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
         const bool staged = sm.staged != 0;
         if (COND != MFREE_COND_PSE && threadIdx.x == 0) {  // read by the targets after the next barrier
             float4 org = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (!a.p.full_stencil && !a.clk->prune_off) {
+            const float md = __uint_as_float(a.clk->max_disp);
+            if (!a.p.full_stencil && md <= PRUNE_DISP_MAX) {
                 const float *gm = a.p.grid_moving ? a.clk->grid_min : a.p.grid_min0;
-                org = make_float4(gm[0], gm[1], gm[2], 1.f);
+                org = make_float4(gm[0], gm[1], gm[2], md + PRUNE_SLACK);
             }
             sm.org = org;
         }

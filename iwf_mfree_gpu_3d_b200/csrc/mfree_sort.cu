@@ -43,7 +43,7 @@ __device__ __forceinline__ void clock_body(const StepArgs &a, int record_mode) {
         c->parity ^= 1;      // the last step's output is this step's input
     }
     c->pending = 1;
-    c->prune_off = 0;
+    c->max_disp = 0u;
     const float t = c->t;
     c->record = record_mode == 1 ? 1
                 : record_mode == 2 ? (P.record_every > 0 && (c->step_index % P.record_every) == 0)
@@ -365,10 +365,17 @@ template <bool PREC> __device__ __forceinline__ void gather_predict_body(const S
     if (i >= N) return;  // blanked: frozen
     const float h2 = 0.5f * P.dt;
     HalfStep hs = half_step<PREC>(h2, pos, vel, sa, sb, da, dv, dsa, dsb, lo, lob);
-    {   // the pair kernel's stencil pruning assumes a move of at most PRUNE_DISP cells
-        const float lim = PRUNE_DISP * P.gdx;
-        if (!(fabsf(hs.x - pos.x) <= lim && fabsf(hs.y - pos.y) <= lim && fabsf(hs.z - pos.z) <= lim))
-            if (atomicExch(&a.clk->prune_off, 1) == 0) atomicAdd(&a.clk->full_stencil_steps, 1ull);
+    {   // the step's largest predictor move in cells (the pair kernel's pruning margin): a
+        // warp maximum, raised in the clock only when it is larger than the value there
+        float d = fmaxf(fabsf(hs.x - pos.x), fmaxf(fabsf(hs.y - pos.y), fabsf(hs.z - pos.z))) / P.gdx;
+        if (!(d <= PRUNE_DISP_MAX)) d = 2.0f * PRUNE_DISP_MAX;  // NaN, Inf or beyond the cap
+        const unsigned act = __activemask();
+        const unsigned m = __reduce_max_sync(act, __float_as_uint(d));  // d >= 0: bits order as values
+        if ((threadIdx.x & 31) == __ffs(act) - 1 && m > *(volatile unsigned *)&a.clk->max_disp) {
+            const unsigned cap = __float_as_uint(PRUNE_DISP_MAX);
+            const unsigned old = atomicMax(&a.clk->max_disp, m);
+            if (m > cap && old <= cap) atomicAdd(&a.clk->full_stencil_steps, 1ull);  // once per step
+        }
     }
     const bool tool = fc.w == 1.f;
     float prs = 0.f;

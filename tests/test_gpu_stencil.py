@@ -42,17 +42,30 @@ def test_pruned_stencil_equals_full_stencil(cspm, conduction):
     assert cb["full_stencil_steps"] == 0
 
 
-def test_fast_particles_switch_the_step_to_the_full_stencil():
-    """A few particles at 3000 m/s move ~3 % of a cell in the predictor's half
-    step, more than the pruning's margin: those steps use the full stencil."""
-    sc = scenes.orthogonal_cutting(30, 15, 12)
-
+def _kick(speed):
     def kick(sim):
         v = sim.get("VEL").reshape(-1, 4).copy()
-        v[:: 997, 0] = 0.3  # cm/us
+        v[:: 997, 0] = speed  # cm/us
         sim.set("VEL", v)
+    return kick
 
-    (fa, ca), (fb, _) = _pair(sc, 3, setup=kick)
+
+def test_fast_particles_widen_the_pruning_margin():
+    """A few particles at 3000 m/s move ~5 % of a cell in the predictor's half
+    step: the margin grows with the step's largest move and the fields stay
+    those of the full stencil."""
+    sc = scenes.orthogonal_cutting(30, 15, 12)
+    (fa, ca), (fb, _) = _pair(sc, 3, setup=_kick(0.3))
+    _assert_identical(fa, fb)
+    assert ca["full_stencil_steps"] == 0
+
+
+def test_very_fast_particles_switch_the_step_to_the_full_stencil():
+    """Particles at 30 km/s move about half a cell in the half step, beyond
+    the largest margin the pruning takes: those steps use the full stencil
+    and are counted."""
+    sc = scenes.orthogonal_cutting(30, 15, 12)
+    (fa, ca), (fb, _) = _pair(sc, 3, setup=_kick(3.0))
     _assert_identical(fa, fb)
     assert ca["full_stencil_steps"] >= 1
 
