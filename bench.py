@@ -470,6 +470,7 @@ def run_e2e(sc, args, opts, dist, local_rank) -> dict:
     t0 = time.perf_counter()
     s = api.Simulation(host["pos"], host["vel"], host["rho"], host["h"], T=host["T"], fixed=host["fixed"],
                        tool_p=host["tool_p"])
+    t_create = time.perf_counter()
     s.set_physics(**sc.phys)
     s.set_correctors(**sc.corr)
     if sc.joco:
@@ -486,18 +487,29 @@ def run_e2e(sc, args, opts, dist, local_rank) -> dict:
     dt = np.float32(sc.dt)
     s.set_time(float(dt), float(dt))
     d2h = 0
+    t_setup = time.perf_counter()
+    marks = []
     for _ in range(args.steps):
         s.advance(1, record_every=1, use_graph=True)  # one replay of the captured step, forces recorded
         f = s.tool_forces()  # the step's result, read back every step
         d2h += f.nbytes
+        if len(marks) < 1:
+            marks.append(time.perf_counter())
+    t_steps = time.perf_counter()
+    if not marks:
+        marks.append(t_steps)
     out = [s.get(n, out=res[n]) for n in names]
     d2h += sum(a.nbytes for a in out)
-    t = time.perf_counter() - t0
+    t_end = time.perf_counter()
+    t = t_end - t0
+    phases = {"create": t_create - t0, "setup": t_setup - t_create, "first_step": marks[0] - t_setup,
+              "other_steps": t_steps - marks[0], "read_back": t_end - t_steps}
     s.close()
     t = reduce_max(dist, t, f"cuda:{local_rank}")
     world = dist.get_world_size() if dist else 1
     return {"value": aggregate(sc.n, args.steps, world, t), "unit": "particle-steps/s",
             "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
+            "phases_ms": {k: round(v * 1e3, 2) for k, v in phases.items()},
             "note": "wall clock: context creation from pinned host arrays, setup, steps with a per-step tool-force "
                     "read-back, final read-back of POS/VEL/S/T/EPS_PL into pinned host arrays; state bytes amortised "
                     "over the steps"}
