@@ -171,6 +171,15 @@ int mfree_get_options(const mfree_ctx *ctx, mfree_options *opt);
 int mfree_set_grid(mfree_ctx *ctx, const float bbmin[3], const float bbmax[3], float h);
 /* grid_base::set_bbox_vel (grid_gpu_base.cu:113-115): moving locked grid */
 int mfree_set_grid_velocity(mfree_ctx *ctx, const float vel[3]);
+/* grid_gpu_green(max_cell, num_part) (grid_gpu_green.cu:336-340,
+ * grid_gpu_base.cu:275-278): the unlocked grid.  Before every step the grid
+ * box becomes the bounding box of the active particles (+-1e-6) and the cell
+ * edge their largest h (update_geometry, grid_gpu_base.cu:185-233); a grid of
+ * max_cell cells or more fails the step with MFREE_ERR_ARG (the reference
+ * asserts).  Each step reads the box back to the host, so steps of such a
+ * context run eagerly (mfree_advance does not capture a graph) and the
+ * context cannot join a batch.  mfree_set_grid locks the grid again. */
+int mfree_set_grid_adaptive(mfree_ctx *ctx, long max_cell);
 /* blanking(bbmin, bbmax, [bbvel,] max_vel) (blanking.cpp:29-33) */
 int mfree_set_blanking(mfree_ctx *ctx, const float bbmin[3], const float bbmax[3],
                        const float *bbvel3, float max_vel);

@@ -32,7 +32,7 @@ CONTACT_HASHED, CONTACT_EXHAUSTIVE = 0, 1
 EXPORTS = [
     "mfree_create", "mfree_destroy", "mfree_last_error", "mfree_set_physics", "mfree_set_correctors",
     "mfree_set_johnson_cook", "mfree_set_thermal_workpiece", "mfree_set_thermal_tool", "mfree_set_options",
-    "mfree_get_options", "mfree_set_grid", "mfree_set_grid_velocity", "mfree_set_blanking", "mfree_set_time",
+    "mfree_get_options", "mfree_set_grid", "mfree_set_grid_velocity", "mfree_set_grid_adaptive", "mfree_set_blanking", "mfree_set_time",
     "mfree_get_time", "mfree_add_tool", "mfree_tool_set_birth_death", "mfree_get_tool_forces",
     "mfree_get_tool_info", "mfree_get_tool_normals", "mfree_get_tool_cells", "mfree_step", "mfree_advance",
     "mfree_sync", "mfree_get_counts", "mfree_field_width", "mfree_get_field", "mfree_set_field",
@@ -46,6 +46,7 @@ EXPORTS = [
     "mfree_write_vtk_tools", "mfree_write_vtk_blanking", "mfree_append_force_log", "mfree_export_state",
     "mfree_import_state", "mfree_inject_fault",
 ]
+ERR_ARG = -1
 ERR_BUDGET = -7
 ERR_TIMEOUT = -8
 KERNELS = ["clock", "hash", "scan_reduce", "scan_top", "scan_down", "scatter", "cell_fixup", "gather_predict",
@@ -111,6 +112,7 @@ def lib(path: str = LIB_PATH):
     L.mfree_get_options.argtypes = [P, C.POINTER(Options)]
     L.mfree_set_grid.argtypes = [P, fp, fp, F]
     L.mfree_set_grid_velocity.argtypes = [P, fp]
+    L.mfree_set_grid_adaptive.argtypes = [P, C.c_long]
     L.mfree_set_blanking.argtypes = [P, fp, fp, fp, F]
     L.mfree_set_time.argtypes = [P, F, F]
     L.mfree_get_time.argtypes = [P, fp, fp]
@@ -276,6 +278,10 @@ class Simulation:
         lo, plo = _f32(bbmin)
         hi, phi = _f32(bbmax)
         _check(self.L.mfree_set_grid(self.h, plo, phi, float(h)))
+
+    def set_grid_adaptive(self, max_cell: int):
+        """The unlocked grid (grid_gpu_green(max_cell, N)): box and cell edge from the particles every step."""
+        _check(self.L.mfree_set_grid_adaptive(self.h, int(max_cell)))
 
     def set_grid_velocity(self, vel):
         v, p = _f32(vel)
@@ -499,7 +505,10 @@ class Simulation:
         opts = dict(scene.options)
         opts.update(option_overrides)
         s.set_options(**opts)
-        s.set_grid(scene.grid_bbmin, scene.grid_bbmax, scene.grid_h)
+        if scene.grid_max_cell > 0:
+            s.set_grid_adaptive(scene.grid_max_cell)
+        else:
+            s.set_grid(scene.grid_bbmin, scene.grid_bbmax, scene.grid_h)
         s.set_blanking(scene.blank_bbmin, scene.blank_bbmax, scene.blank_vmax)
         for t in scene.tools:
             s.add_tool(t.verts, t.tris, t.vel, t.contact_alpha, t.mu, t.algorithm)

@@ -264,6 +264,7 @@ int mfree_batch_destroy(mfree_batch *b) {
 int mfree_batch_admit(mfree_batch *b, mfree_ctx *c, long long steps, int *slot) {
     if (!b || !c) return fail(MFREE_ERR_ARG, "mfree_batch_admit: null argument");
     if (c->owner) return fail(MFREE_ERR_ARG, "mfree_batch_admit: the context already belongs to a batch");
+    if (c->grid_adaptive) return fail(MFREE_ERR_ARG, "mfree_batch_admit: a context with an unlocked grid steps alone");
     if (c->device != b->device) return fail(MFREE_ERR_ARG, "mfree_batch_admit: the context is on another device");
     int st = ready(c);
     if (st) return st;

@@ -60,6 +60,9 @@ struct mfree_ctx {
     bool grid_set = false;
     float g_bbmin[3], g_bbmax[3], g_dx = 0.f, g_vel[3] = {0, 0, 0};
     long nx = 0, ny = 0, nz = 0, num_cell = 0;
+    bool grid_adaptive = false;  // unlocked grid: box and cell edge from the particles every step
+    long max_cell = 0;           // its cell limit (the scratch is sized for it)
+    int *d_bbox = nullptr, *h_bbox = nullptr;  // its bounding-box reduction (device, page-locked host)
     bool blank_set = false;
     float b_min[3], b_max[3], b_vel[3] = {0, 0, 0}, b_vmax = 0.f;
     float dt = 0.f, t = 0.f;

@@ -111,7 +111,7 @@ Params make_params(const mfree_ctx *c) {
     P.gnz = int(c->nz);
     P.num_cell = int(c->num_cell);
     P.gdx = c->g_dx;
-    P.grid_moving = (c->g_vel[0] != 0.f || c->g_vel[1] != 0.f || c->g_vel[2] != 0.f) ? 1 : 0;
+    P.grid_moving = !c->grid_adaptive && (c->g_vel[0] != 0.f || c->g_vel[1] != 0.f || c->g_vel[2] != 0.f) ? 1 : 0;
     for (int d = 0; d < 3; d++) {
         P.grid_vel[d] = c->g_vel[d];
         P.grid_min0[d] = c->g_bbmin[d];
@@ -174,18 +174,20 @@ StepArgs make_args(mfree_ctx *c) {
 
 // scratch that depends on the grid size
 int ensure_scratch(mfree_ctx *c) {
-    if (c->scratch_cells == size_t(c->num_cell) && !c->scratch_allocs.empty()) return MFREE_OK;
+    // an unlocked grid changes its cell count every step: its scratch holds max_cell cells
+    const long cells = c->grid_adaptive ? c->max_cell : c->num_cell;
+    if (c->scratch_cells == size_t(cells) && !c->scratch_allocs.empty()) return MFREE_OK;
     free_list(c->scratch_allocs);
     c->scratch_bytes = 0;
     auto &L = c->scratch_allocs;
     int st;
-    if ((st = dalloc(c, &c->scr.count, c->num_cell + 1, L))) return st;
-    if ((st = dalloc(c, &c->scr.first, c->num_cell + 2 + SCAN_TILE, L))) return st;
-    if ((st = dalloc(c, &c->scr.tile_sum, scan_tiles(c) + 1, L))) return st;
+    if ((st = dalloc(c, &c->scr.count, cells + 1, L))) return st;
+    if ((st = dalloc(c, &c->scr.first, cells + 2 + SCAN_TILE, L))) return st;
+    if ((st = dalloc(c, &c->scr.tile_sum, (cells + 1 + SCAN_TILE - 1) / SCAN_TILE + 1, L))) return st;
     // the pair kernel's tile list: a tile of any depth holds a cell at least
-    if ((st = dalloc(c, &c->d_tiles, c->num_cell + 1, L))) return st;
-    CUDA_TRY(cudaMemsetAsync(c->scr.count, 0, sizeof(int) * (c->num_cell + 1), c->stream));
-    c->scratch_cells = size_t(c->num_cell);
+    if ((st = dalloc(c, &c->d_tiles, cells + 1, L))) return st;
+    CUDA_TRY(cudaMemsetAsync(c->scr.count, 0, sizeof(int) * (cells + 1), c->stream));
+    c->scratch_cells = size_t(cells);
     invalidate_graphs(c);
     return MFREE_OK;
 }
@@ -482,6 +484,8 @@ int clone_ctx(const mfree_ctx *src, cudaStream_t s, std::unique_ptr<mfree_ctx> &
     c->ny = src->ny;
     c->nz = src->nz;
     c->num_cell = src->num_cell;
+    c->grid_adaptive = src->grid_adaptive;
+    c->max_cell = src->max_cell;
     c->blank_set = src->blank_set;
     c->b_vmax = src->b_vmax;
     c->dt = src->dt;
@@ -578,6 +582,7 @@ int mfree_destroy(mfree_ctx *c) {
     for (auto e : c->timer)
         if (e) cudaEventDestroy(e);
     if (c->h_nact) cudaFreeHost(c->h_nact);
+    if (c->h_bbox) cudaFreeHost(c->h_bbox);
     if (c->nact_ev) cudaEventDestroy(c->nact_ev);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -646,6 +651,22 @@ int mfree_set_grid(mfree_ctx *c, const float bbmin[3], const float bbmax[3], flo
     long nc = c->nx * c->ny * c->nz;
     if (nc >= long(INT_MAX) / 2) return fail(MFREE_ERR_ARG, "grid has too many cells");
     c->num_cell = nc;
+    c->grid_set = true;
+    c->grid_adaptive = false;
+    c->clock_dirty = true;
+    invalidate_graphs(c);
+    return MFREE_OK;
+}
+int mfree_set_grid_adaptive(mfree_ctx *c, long max_cell) {
+    if (!c || max_cell < 2 || max_cell >= long(INT_MAX) / 2) return fail(MFREE_ERR_ARG, "mfree_set_grid_adaptive: bad arguments");
+    if (c->owner) return fail(MFREE_ERR_ARG, "mfree_set_grid_adaptive: the context belongs to a batch");
+    c->grid_adaptive = true;
+    c->max_cell = max_cell;
+    // a placeholder grid until the first step bounds the particles
+    c->nx = c->ny = c->nz = 1;
+    c->num_cell = 1;
+    c->g_dx = 0.f;
+    for (int d = 0; d < 3; d++) c->g_bbmin[d] = c->g_bbmax[d] = 0.f;
     c->grid_set = true;
     c->clock_dirty = true;
     invalidate_graphs(c);
@@ -782,12 +803,107 @@ int mfree_get_tool_cells(mfree_ctx *c, int k, int *cells, int *boxed_src) {
     return MFREE_OK;
 }
 
+// Bounding box of the first n particles of the current order and their
+// largest h (update_geometry's unlocked branch, grid_gpu_base.cu:185-204; n =
+// the active count when blanking is on, as particles->N, else n_init).
+// Floats are reduced as order-preserving int keys, so atomicMin/atomicMax give
+// the exact extremes; NaN coordinates are left out.
+__device__ __forceinline__ int float_key(float f) {
+    const int b = __float_as_int(f);
+    return b >= 0 ? b : b ^ 0x7fffffff;
+}
+float key_float(int k) {
+    const int b = k >= 0 ? k : k ^ 0x7fffffff;
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f;
+}
+__global__ void k_bbox_init(int *out) {
+    if (threadIdx.x < 7) out[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;  // min xyz, max xyz, max h
+}
+__global__ void __launch_bounds__(256) k_bbox(const float4 *pos, int n_init, const DevClock *clk, int use_active,
+                                              int *out) {
+    const int n = use_active ? min(clk->n_active, n_init) : n_init;
+    int k[7] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN, INT_MIN};
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) {
+        const float4 p = pos[i];
+        const float v[4] = {p.x, p.y, p.z, p.w};
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+            if (!isnan(v[d])) {
+                k[d] = min(k[d], float_key(v[d]));
+                k[3 + d] = max(k[3 + d], float_key(v[d]));
+            }
+        if (!isnan(p.w)) k[6] = max(k[6], float_key(p.w));
+    }
+#pragma unroll
+    for (int d = 0; d < 7; d++) k[d] = d < 3 ? __reduce_min_sync(0xffffffffu, k[d]) : __reduce_max_sync(0xffffffffu, k[d]);
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int d = 0; d < 7; d++) {
+            if (d < 3) atomicMin(out + d, k[d]);
+            else atomicMax(out + d, k[d]);
+        }
+    }
+}
+
+// the unlocked grid of this step from the particles (grid_gpu_base.cu:185-233),
+// in the reference's float arithmetic
+int adapt_grid(mfree_ctx *c) {
+    if (!c->d_bbox) {
+        int st = dalloc(c, &c->d_bbox, 8, c->allocs);
+        if (st) return st;
+        CUDA_TRY(cudaMallocHost(&c->h_bbox, 8 * sizeof(int)));
+    }
+    const int blocks = std::max(1, std::min((c->n_init + 255) / 256, 4 * c->num_sms));
+    k_bbox_init<<<1, 32, 0, c->stream>>>(c->d_bbox);
+    k_bbox<<<blocks, 256, 0, c->stream>>>(c->st[c->cur].pos4, c->n_init, c->d_clk, c->blank_set ? 1 : 0, c->d_bbox);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(c->h_bbox, c->d_bbox, 7 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (c->h_bbox[0] == INT_MAX || c->h_bbox[6] == INT_MIN)
+        return fail(MFREE_ERR_EMPTY, "the unlocked grid has no particle to bound");
+    float bbmin[3], bbmax[3];
+    for (int d = 0; d < 3; d++) {
+        bbmin[d] = float(double(key_float(c->h_bbox[d])) - 1e-6);
+        bbmax[d] = float(double(key_float(c->h_bbox[3 + d])) + 1e-6);
+    }
+    const float kernel_width = 2.f;
+    const float dx = key_float(c->h_bbox[6]) * kernel_width / 2;
+    long n3[3];
+    for (int d = 0; d < 3; d++) {
+        const float l = bbmax[d] - bbmin[d];
+        const float q = std::ceil(l / dx);
+        if (!(q >= 1.f && q < 1e9f)) return fail(MFREE_ERR_ARG, "the unlocked grid has an unusable size");
+        n3[d] = long(q);
+    }
+    const long nc = n3[0] * n3[1] * n3[2];
+    if (nc >= c->max_cell)
+        return fail(MFREE_ERR_ARG, "the unlocked grid needs " + std::to_string(nc) + " cells, max_cell is " +
+                                       std::to_string(c->max_cell) + " (grid_gpu_base.cu:227-232 asserts)");
+    bool same = dx == c->g_dx && n3[0] == c->nx && n3[1] == c->ny && n3[2] == c->nz;
+    for (int d = 0; d < 3; d++) same = same && bbmin[d] == c->g_bbmin[d] && bbmax[d] == c->g_bbmax[d];
+    if (same) return MFREE_OK;
+    for (int d = 0; d < 3; d++) {
+        c->g_bbmin[d] = bbmin[d];
+        c->g_bbmax[d] = bbmax[d];
+    }
+    c->g_dx = dx;
+    c->nx = n3[0];
+    c->ny = n3[1];
+    c->nz = n3[2];
+    c->num_cell = nc;
+    invalidate_graphs(c);  // the step arguments hold the grid: the table is written again
+    return MFREE_OK;
+}
+
 int mfree_step(mfree_ctx *c, int record_forces) {
     if (!c) return fail(MFREE_ERR_ARG, "null context");
     if (c->owner) return fail(MFREE_ERR_ARG, "mfree_step: the context belongs to a batch (mfree_batch_step steps it)");
     int st = ready(c);
     if (st) return st;
     if ((st = check_empty(c, false))) return st;
+    if (c->grid_adaptive && (st = adapt_grid(c))) return st;
     if ((st = enqueue_step(c, record_forces ? 1 : 0, 0, c->timing))) return st;
     if ((st = note_active_count(c))) return st;
     c->cur ^= 1;
@@ -803,9 +919,10 @@ int mfree_advance(mfree_ctx *c, int nsteps, int record_every, int use_graph) {
     int st = ready(c);
     if (st) return st;
     if ((st = check_empty(c, false))) return st;
-    if (!use_graph) {
+    if (!use_graph || c->grid_adaptive) {  // an unlocked grid is read back before every step: no graph
         for (int k = 0; k < nsteps; k++) {
             const bool rec = record_every > 0 && (c->steps % record_every) == 0;
+            if (c->grid_adaptive && (st = adapt_grid(c))) return st;
             if ((st = enqueue_step(c, rec ? 1 : 0, 0))) return st;
             c->cur ^= 1;
             if (c->pending) c->t = c->t + c->dt;

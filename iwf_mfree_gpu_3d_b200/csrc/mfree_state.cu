@@ -22,7 +22,7 @@ using namespace mfree::host;
 namespace {
 
 constexpr char MAGIC[8] = {'M', 'F', 'R', 'E', 'E', 'S', 'T', '1'};
-constexpr uint32_t VERSION = 1;
+constexpr uint32_t VERSION = 2;
 constexpr int NSTATE = 13;
 
 struct Header {
@@ -43,6 +43,7 @@ struct Config {
     int32_t plastic, grid_set, blank_set, time_set, pending, cur;
     float g_bbmin[3], g_bbmax[3], g_dx, g_vel[3];
     int64_t nx, ny, nz, num_cell;
+    int64_t grid_adaptive, max_cell;
     float b_min[3], b_max[3], b_vel[3], b_vmax;
     float dt, t;
     int64_t steps;
@@ -127,6 +128,8 @@ int mfree_export_state(mfree_ctx *c, void *buf, size_t *size) {
     g.ny = c->ny;
     g.nz = c->nz;
     g.num_cell = c->num_cell;
+    g.grid_adaptive = c->grid_adaptive ? 1 : 0;
+    g.max_cell = c->max_cell;
     g.b_vmax = c->b_vmax;
     g.dt = c->dt;
     g.t = c->t;
@@ -213,6 +216,8 @@ int mfree_import_state(const void *buf, size_t size, void *stream, mfree_ctx **o
     c->ny = long(g.ny);
     c->nz = long(g.nz);
     c->num_cell = long(g.num_cell);
+    c->grid_adaptive = g.grid_adaptive != 0;
+    c->max_cell = long(g.max_cell);
     c->b_vmax = g.b_vmax;
     for (uint32_t k = 0; k < h.num_tools; k++) {
         ToolRec tr{};

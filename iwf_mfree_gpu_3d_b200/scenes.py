@@ -85,6 +85,7 @@ class Scene:
     blank_vmax: float
     dt: float
     tools: List[Tool]
+    grid_max_cell: int = 0     # > 0: unlocked grid (box and cell edge from the particles every step)
 
     @property
     def n(self) -> int:

@@ -72,6 +72,7 @@ def lib():
         L.orc_set_params.argtypes = [P, P, P, P, P, P, P]
         L.orc_set_grid.argtypes = [P, fp, fp, F]
         L.orc_set_grid_velocity.argtypes = [P, fp]
+        L.orc_set_grid_adaptive.argtypes = [P, C.c_long]
         L.orc_set_blanking.argtypes = [P, fp, fp, fp, F]
         L.orc_set_time.argtypes = [P, D, D]
         L.orc_get_time.argtypes = [P]
@@ -195,7 +196,10 @@ class Oracle:
                          C.byref(self._ttool), C.byref(self._opt))
         lo, plo = _f32(scene.grid_bbmin)
         hi, phi = _f32(scene.grid_bbmax)
-        L.orc_set_grid(self.h, plo, phi, scene.grid_h)
+        if getattr(scene, "grid_max_cell", 0) > 0:
+            L.orc_set_grid_adaptive(self.h, int(scene.grid_max_cell))
+        else:
+            L.orc_set_grid(self.h, plo, phi, scene.grid_h)
         blo, pblo = _f32(scene.blank_bbmin)
         bhi, pbhi = _f32(scene.blank_bbmax)
         L.orc_set_blanking(self.h, pblo, pbhi, None, scene.blank_vmax)

@@ -644,6 +644,8 @@ template <class R> struct Sim {
     R g_bbmin[3], g_bbmax[3], g_bbmin0[3], g_bbmax0[3], g_dx;
     long g_nx, g_ny, g_nz, g_ncell;
     V3<R> g_vel;
+    bool g_adaptive = false;  // unlocked grid (grid_gpu_green(max_cell, N))
+    long g_max_cell = 0;
     std::vector<int> cell_start, cell_end;
     // blanking (blanking.cpp)
     bool blank_set = false;
@@ -702,8 +704,20 @@ template <class R> struct Sim {
         g_ncell = g_nx * g_ny * g_nz;
         g_vel = V3<R>(0, 0, 0);
         grid_set = true;
+        g_adaptive = false;
         cell_start.assign(g_ncell, -1);
         cell_end.assign(g_ncell, -1);
+    }
+    void set_grid_adaptive(long max_cell) {
+        g_adaptive = true;
+        g_max_cell = max_cell;
+        g_nx = g_ny = g_nz = g_ncell = 1;
+        g_dx = 0;
+        for (int d = 0; d < 3; d++) g_bbmin[d] = g_bbmin0[d] = g_bbmax[d] = g_bbmax0[d] = 0;
+        g_vel = V3<R>(0, 0, 0);
+        grid_set = true;
+        cell_start.assign(1, -1);
+        cell_end.assign(1, -1);
     }
 
     // ---- do_blanking (actions_gpu.cu:489-531) ----
@@ -736,9 +750,53 @@ template <class R> struct Sim {
         int iz = int((q.z - g_bbmin[2]) / g_dx);
         return int(long(ix) * g_ny * g_nz + long(iy) * g_nz + long(iz));
     }
+    // update_geometry, unlocked branch (grid_gpu_base.cu:185-233): the box of
+    // the first N particles of the current order (+-1e-6) and their largest h
+    // as the cell edge, in the arithmetic of the build (R); NaN coordinates are
+    // left out
+    int adapt_grid() {
+        R mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0}, mh = 0;
+        bool seen[3] = {false, false, false}, seen_h = false;
+        for (int i = 0; i < N; i++) {
+            const R v[3] = {pos[i].x, pos[i].y, pos[i].z};
+            for (int d = 0; d < 3; d++) {
+                if (std::isnan(v[d])) continue;
+                if (!seen[d] || v[d] < mn[d]) mn[d] = v[d];
+                if (!seen[d] || v[d] > mx[d]) mx[d] = v[d];
+                seen[d] = true;
+            }
+            if (!std::isnan(h[i]) && (!seen_h || h[i] > mh)) {
+                mh = h[i];
+                seen_h = true;
+            }
+        }
+        if (!seen[0] || !seen[1] || !seen[2] || !seen_h) return MFREE_ERR_EMPTY;
+        for (int d = 0; d < 3; d++) {
+            g_bbmin[d] = R(double(mn[d]) - 1e-6);
+            g_bbmax[d] = R(double(mx[d]) + 1e-6);
+        }
+        const R kernel_width = 2;
+        g_dx = mh * kernel_width / 2;
+        long n3[3];
+        for (int d = 0; d < 3; d++) {
+            const R l = g_bbmax[d] - g_bbmin[d];
+            n3[d] = long(std::ceil(l / g_dx));
+        }
+        g_nx = n3[0]; g_ny = n3[1]; g_nz = n3[2];
+        g_ncell = g_nx * g_ny * g_nz;
+        if (g_ncell >= g_max_cell || g_ncell <= 0) return MFREE_ERR_ARG;  // the reference asserts
+        cell_start.assign(g_ncell, -1);
+        cell_end.assign(g_ncell, -1);
+        return MFREE_OK;
+    }
+
     int sort_and_cells() {
+        if (g_adaptive) {
+            int st = adapt_grid();
+            if (st) return st;
+        }
         // update_geometry, locked branch (grid_gpu_base.cu:166-183)
-        if (g_vel.x != 0 || g_vel.y != 0 || g_vel.z != 0)
+        if (!g_adaptive && (g_vel.x != 0 || g_vel.y != 0 || g_vel.z != 0))
             for (int d = 0; d < 3; d++) {
                 g_bbmin[d] = g_bbmin0[d] + t * g_vel[d];
                 g_bbmax[d] = g_bbmax0[d] + t * g_vel[d];
@@ -1275,6 +1333,9 @@ int orc_set_params(void *hp, const mfree_phys *phys, const mfree_corr *corr, con
 }
 int orc_set_grid(void *hp, const float *bbmin, const float *bbmax, float h) {
     return with_sim((Handle *)hp, [&](auto &s) { s.set_grid(bbmin, bbmax, h); return 0; });
+}
+int orc_set_grid_adaptive(void *hp, long max_cell) {
+    return with_sim((Handle *)hp, [&](auto &s) { s.set_grid_adaptive(max_cell); return 0; });
 }
 int orc_set_grid_velocity(void *hp, const float *v) {
     return with_sim((Handle *)hp, [&](auto &s) { s.g_vel = {v[0], v[1], v[2]}; return 0; });

@@ -66,3 +66,17 @@ def compare(g: dict, o: dict, scene, names=FIELDS) -> dict:
         res[n] = rel_l2(a, b, mask)
     res["blank_mismatch"] = int(((g["BLANKED"] != 0) != (o["BLANKED"] != 0)).sum())
     return res
+
+
+def unlocked_grid(pos4: np.ndarray, h: np.ndarray, n: int):
+    """The unlocked grid of grid_base::update_geometry (grid_gpu_base.cu:185-233)
+    in the reference's FP32 arithmetic: the box of the first n particles
+    +-1e-6 (float minus a double literal, stored as float), the largest h as
+    the cell edge, ceil(length / edge) cells per axis."""
+    p = np.asarray(pos4, np.float32)[:n, :3]
+    mn, mx = p.min(axis=0), p.max(axis=0)
+    bbmin = (mn.astype(np.float64) - 1e-6).astype(np.float32)
+    bbmax = (mx.astype(np.float64) + 1e-6).astype(np.float32)
+    dx = np.float32(np.asarray(h, np.float32)[:n].max()) * np.float32(2.0) / np.float32(2.0)
+    n3 = tuple(int(np.ceil(np.float32(bbmax[d] - bbmin[d]) / dx)) for d in range(3))
+    return n3, bbmin, np.float32(dx)

@@ -106,3 +106,37 @@ def test_tool_setup_oracle_wedge():
     assert np.all(np.einsum("ij,ij->i", nrm[:, 0], centre - fc) > 0)
     cells, src = o.tool_cells()
     assert cells[-1] == info["num_boxed"] and set(src) == set(range(12))
+
+
+def test_oracle_unlocked_grid_follows_the_particles():
+    """grid_gpu_green(max_cell, N): the oracle's grid after a step is the
+    bounding box of the particles at its start (FP32 build arithmetic), and
+    the FP32 and FP64 oracles with an unlocked grid still agree."""
+    from helpers import unlocked_grid
+    sc = scenes.orthogonal_cutting(16, 8, 6)
+    sc.grid_max_cell = 100000
+    b = oracle.Oracle(sc, prec=32)
+    b.step()
+    n3, bbmin, dx = unlocked_grid(sc.pos, sc.h, sc.n)
+    g_n3, g_lo, g_dx = b.grid()
+    assert tuple(int(v) for v in g_n3) == n3
+    np.testing.assert_array_equal(np.float32(g_lo), bbmin)
+    assert np.float32(g_dx) == dx
+    a = oracle.Oracle(sc, prec=64)
+    a.step()
+    for _ in range(15):
+        a.step()
+        b.step()
+    ia, ib = a.field("ID").astype(int), b.field("ID").astype(int)
+    pa = np.empty((sc.n, 4)); pa[ia] = a.field("POS")
+    pb = np.empty((sc.n, 4)); pb[ib] = b.field("POS")
+    d0 = sc.pos[:, :3]
+    assert np.linalg.norm((pa - pb)[:, :3]) / np.linalg.norm(pa[:, :3] - d0) < 1e-2
+
+
+def test_oracle_unlocked_grid_beyond_max_cell_fails():
+    sc = scenes.orthogonal_cutting(16, 8, 6)
+    sc.grid_max_cell = 100
+    o = oracle.Oracle(sc, prec=32)
+    with pytest.raises(RuntimeError):
+        o.step()
