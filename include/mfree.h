@@ -115,6 +115,28 @@ enum mfree_field {
     MFREE_NUM_FIELDS
 };
 
+/* ---- compact structure-of-arrays access ----------------------------------
+ * The library's own particle arrays: n_init float4 entries each, current
+ * sorted order, the deviatoric stress as its 6 independent components (no
+ * counterpart in the reference, whose particle_gpu keeps one array per field;
+ * one copy instead of a per-field conversion). */
+enum mfree_array {
+    MFREE_A_POS_H = 0,    /* (x, y, z, h)                                      */
+    MFREE_A_VEL_RHO,      /* (vx, vy, vz, rho)                                 */
+    MFREE_A_S_A,          /* (Sxx, Syy, Szz, Sxy)                              */
+    MFREE_A_S_B,          /* (Sxz, Syz, T, eps_pl)                             */
+    MFREE_A_POS_T,        /* (xdot, ydot, zdot, rho_t)                         */
+    MFREE_A_VEL_T,        /* (vx_t, vy_t, vz_t, T_t)                           */
+    MFREE_A_S_T_A,        /* (Sxx_t, Syy_t, Szz_t, Sxy_t)                      */
+    MFREE_A_S_T_B,        /* (Sxz_t, Syz_t, eps_pl_dot, fixed)                 */
+    MFREE_A_FC,           /* (fc.x, fc.y, fc.z, tool_particle)                 */
+    MFREE_A_FT,           /* (ft.x, ft.y, ft.z, blanked)                       */
+    MFREE_A_VEL_BC,       /* (vbc.x, vbc.y, vbc.z, id as int bits)             */
+    MFREE_A_LO,           /* precision form: (x_lo, y_lo, z_lo, vx_lo)         */
+    MFREE_A_LO_B,         /* precision form: (vy_lo, vz_lo, 0, 0)              */
+    MFREE_NUM_ARRAYS
+};
+
 /* per-context counters of device-detected conditions */
 typedef struct {
     int64_t steps;              /* steps taken                                          */
@@ -241,6 +263,14 @@ int mfree_set_field(mfree_ctx *ctx, int field, const void *in);
 /* the same in double: MFREE_POS and MFREE_VEL return hi + lo of the
  * compensated accumulation when options.precision = 1 */
 int mfree_get_field_f64(mfree_ctx *ctx, int field, double *out);
+/* the compact arrays (enum mfree_array): copy one array (4 * n_init floats)
+ * to / from host memory */
+int mfree_get_array(mfree_ctx *ctx, int array, float *out4);
+int mfree_set_array(mfree_ctx *ctx, int array, const float *in4);
+/* the device address of the array's current copy, for callers that read it
+ * on the device in stream order; valid until the next step (each step writes
+ * the other of two copies) */
+int mfree_array_device_ptr(mfree_ctx *ctx, int array, void **dptr);
 /* cell ranges in the reference format (cell_start/cell_end, -1 = empty;
  * grid_gpu_green.cu:24-70,277-278), num_cell entries each */
 int mfree_get_cells(mfree_ctx *ctx, int *cell_start, int *cell_end);

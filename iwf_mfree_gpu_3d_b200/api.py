@@ -44,8 +44,9 @@ EXPORTS = [
     "mfree_batch_get_tiling", "mfree_batch_autotune", "mfree_batch_sync", "mfree_batch_timer_start",
     "mfree_batch_timer_stop", "mfree_device_bytes", "mfree_scene_bytes", "mfree_write_vtk", "mfree_output_wait",
     "mfree_write_vtk_tools", "mfree_write_vtk_blanking", "mfree_append_force_log", "mfree_export_state",
-    "mfree_import_state", "mfree_inject_fault",
+    "mfree_import_state", "mfree_inject_fault", "mfree_get_array", "mfree_set_array", "mfree_array_device_ptr",
 ]
+ARRAYS = ["POS_H", "VEL_RHO", "S_A", "S_B", "POS_T", "VEL_T", "S_T_A", "S_T_B", "FC", "FT", "VEL_BC", "LO", "LO_B"]
 ERR_ARG = -1
 ERR_BUDGET = -7
 ERR_TIMEOUT = -8
@@ -113,6 +114,9 @@ def lib(path: str = LIB_PATH):
     L.mfree_set_grid.argtypes = [P, fp, fp, F]
     L.mfree_set_grid_velocity.argtypes = [P, fp]
     L.mfree_set_grid_adaptive.argtypes = [P, C.c_long]
+    L.mfree_get_array.argtypes = [P, I, fp]
+    L.mfree_set_array.argtypes = [P, I, fp]
+    L.mfree_array_device_ptr.argtypes = [P, I, C.POINTER(P)]
     L.mfree_set_blanking.argtypes = [P, fp, fp, fp, F]
     L.mfree_set_time.argtypes = [P, F, F]
     L.mfree_get_time.argtypes = [P, fp, fp]
@@ -404,6 +408,26 @@ class Simulation:
                              f"{self.n_init * w} entries")
         _check(self.L.mfree_get_field(self.h, f, out.ctypes.data_as(C.c_void_p)))
         return out.reshape(self.n_init, w) if w > 1 else out.reshape(-1)
+
+    def get_array(self, name: str, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """One of the library's own float4 arrays (ARRAYS), n_init x 4."""
+        if out is None:
+            out = np.empty((self.n_init, 4), np.float32)
+        elif out.dtype != np.float32 or out.size != 4 * self.n_init or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"get_array({name!r}): out must be a C-contiguous float32 array of {4 * self.n_init}")
+        _check(self.L.mfree_get_array(self.h, ARRAYS.index(name), out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out.reshape(self.n_init, 4)
+
+    def set_array(self, name: str, values):
+        a = np.ascontiguousarray(values, dtype=np.float32).reshape(-1)
+        if a.size != 4 * self.n_init:
+            raise ValueError(f"set_array({name!r}): {4 * self.n_init} floats expected")
+        _check(self.L.mfree_set_array(self.h, ARRAYS.index(name), a.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def array_device_ptr(self, name: str) -> int:
+        p = C.c_void_p()
+        _check(self.L.mfree_array_device_ptr(self.h, ARRAYS.index(name), C.byref(p)))
+        return int(p.value or 0)
 
     def get64(self, name: str) -> np.ndarray:
         f = FIELD_ID[name]

@@ -1375,6 +1375,40 @@ int mfree_set_field(mfree_ctx *c, int f, const void *in) {
     }
 }
 
+namespace {
+float4 *state_array(mfree_ctx *c, int a) {
+    const State &S = c->st[c->cur];
+    float4 *const arr[MFREE_NUM_ARRAYS] = {S.pos4, S.vel4, S.sa4, S.sb4, S.da4,  S.dv4,  S.dsa4,
+                                           S.dsb4, S.fc4,  S.ft4, S.bc4, S.lo4, S.lo4b};
+    return a >= 0 && a < MFREE_NUM_ARRAYS ? arr[a] : nullptr;
+}
+}  // namespace
+
+int mfree_get_array(mfree_ctx *c, int a, float *out4) {
+    if (!c || !out4) return fail(MFREE_ERR_ARG, "null argument");
+    float4 *src = state_array(c, a);
+    if (!src) return fail(MFREE_ERR_ARG, "mfree_get_array: unknown array");
+    CUDA_TRY(cudaMemcpyAsync(out4, src, sizeof(float4) * size_t(c->n_init), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return MFREE_OK;
+}
+int mfree_set_array(mfree_ctx *c, int a, const float *in4) {
+    if (!c || !in4) return fail(MFREE_ERR_ARG, "null argument");
+    float4 *dst = state_array(c, a);
+    if (!dst) return fail(MFREE_ERR_ARG, "mfree_set_array: unknown array");
+    invalidate_graphs(c);
+    CUDA_TRY(cudaMemcpyAsync(dst, in4, sizeof(float4) * size_t(c->n_init), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return MFREE_OK;
+}
+int mfree_array_device_ptr(mfree_ctx *c, int a, void **dptr) {
+    if (!c || !dptr) return fail(MFREE_ERR_ARG, "null argument");
+    float4 *p = state_array(c, a);
+    if (!p) return fail(MFREE_ERR_ARG, "mfree_array_device_ptr: unknown array");
+    *dptr = p;
+    return MFREE_OK;
+}
+
 int mfree_get_cells(mfree_ctx *c, int *cs, int *ce) {
     if (!c || !cs || !ce) return fail(MFREE_ERR_ARG, "null argument");
     if (!c->grid_set || c->scratch_allocs.empty()) return fail(MFREE_ERR_ARG, "no step has run");

@@ -216,3 +216,46 @@ def test_moving_grid_and_blanking_box():
     err = compare(gpu_state(sim), oracle_state(orc), sc)
     assert err["blank_mismatch"] == 0
     sim.close()
+
+
+def test_compact_arrays_match_the_reference_layout_fields():
+    """mfree_get_array / mfree_set_array: the library's own float4 arrays hold
+    the same values as the reference-layout fields, and writing a field
+    through either path steps on identically."""
+    sc = scenes.small_scene()
+    sim = api.Simulation.from_scene(sc, precision=1)
+    sim.advance(5, use_graph=True)
+    A = {n: sim.get_array(n).copy() for n in api.ARRAYS}
+    np.testing.assert_array_equal(A["POS_H"][:, :3], sim.get("POS")[:, :3])
+    np.testing.assert_array_equal(A["POS_H"][:, 3], sim.get("H"))
+    np.testing.assert_array_equal(A["VEL_RHO"][:, 3], sim.get("RHO"))
+    S = sim.get("S").reshape(-1, 9)  # GLM column-major m[col][row]
+    np.testing.assert_array_equal(A["S_A"], S[:, [0, 4, 8, 1]])
+    np.testing.assert_array_equal(A["S_B"][:, :2], S[:, [2, 5]])
+    np.testing.assert_array_equal(A["S_B"][:, 2], sim.get("T"))
+    np.testing.assert_array_equal(A["S_B"][:, 3], sim.get("EPS_PL"))
+    np.testing.assert_array_equal(A["S_T_B"][:, 3], sim.get("FIXED"))
+    np.testing.assert_array_equal(A["FC"][:, 3], sim.get("TOOL_PARTICLE"))
+    np.testing.assert_array_equal(A["FT"][:, 3], sim.get("BLANKED"))
+    np.testing.assert_array_equal(A["VEL_BC"][:, 3].view(np.int32), sim.get("ID"))
+    p64 = sim.get64("POS")[:, :3]
+    np.testing.assert_array_equal(p64, A["POS_H"][:, :3].astype(np.float64) + A["LO"][:, :3])
+    ptr = sim.array_device_ptr("POS_H")
+    sim.step()
+    assert ptr != 0 and sim.array_device_ptr("POS_H") != ptr  # the other copy after a step
+
+    a = api.Simulation.from_scene(sc)
+    b = api.Simulation.from_scene(sc)
+    for s in (a, b):
+        s.advance(3, use_graph=True)
+    T = b.get("T") + np.float32(25.0)
+    b.set("T", T)
+    sb = a.get_array("S_B").copy()
+    sb[:, 2] = T
+    a.set_array("S_B", sb)
+    for s in (a, b):
+        s.advance(4, use_graph=True)
+    for name in ("POS", "VEL", "S", "T", "EPS_PL", "ID"):
+        np.testing.assert_array_equal(a.get(name), b.get(name), err_msg=name)
+    for s in (sim, a, b):
+        s.close()
