@@ -225,6 +225,17 @@ def hbm_roofline(rate: float, sc) -> dict:
 
 
 # -------------------------------------------------------------- oracle ----
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), for the baseline's record."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(workload: str, budget_s: float = 20.0) -> dict:
     """FP64 oracle (OpenMP, every host core) on a bounded sample of the workload."""
     import oracle
@@ -240,7 +251,7 @@ def cpu_baseline(workload: str, budget_s: float = 20.0) -> dict:
     for _ in range(nsteps):
         orc.step()
     t = time.perf_counter() - t0
-    return {"value": sc.n * nsteps / t, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+    return {"value": sc.n * nsteps / t, "unit": "particle-steps/s", "cores": cores, "cpu": cpu_model(), "kind": "port",
             "sample": f"{nsteps} FP64 oracle step(s) of the full {sc.n}-particle scene after 1 warm-up step"}
 
 
@@ -280,7 +291,7 @@ def run_reference(args, rank: int, world: int):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference", "config": workload_config(args.workload, sc),
-            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": cores, "cpu": cpu_model(), "kind": "port",
                              "sample": "FP64 oracle restatement of leap_frog::step, " + desc},
             "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
