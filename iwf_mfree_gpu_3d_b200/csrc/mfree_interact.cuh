@@ -517,27 +517,72 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
     const float four_h2 = __fmul_rn(__fmul_rn(4.0f, I.h), I.h);
     int qn = 0;  // in-support neighbours of the target (the group's ballots: the same in every lane)
     float pse = 0.f;
-    scan([&](int j, bool act) {
-        bool ins = false;
-        if (act) {
-            const float4 Pj = rP[j];
-            const float dx = I.x - Pj.x, dy = I.y - Pj.y, dz = I.z - Pj.z;
-            const float r2 = dist2_rn(dx, dy, dz);
-            ins = !(r2 >= four_h2) && (r2 > 9.99999994e-9f);  // in_support()
-            if (COND == MFREE_COND_PSE) {
-                const float2 tv = reinterpret_cast<const float2 *>(rC + j)[1];  // (T_j, V_j)
-                float e2;
-                asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e2) : "f"(pse_k * r2));
-                pse = fmaf((tv.x - I.T) * tv.y, e2, pse);
+    {   // two candidates per lane and iteration (k and k + LPP): both column
+        // walks, then both loads, then the arithmetic, so the shared-memory
+        // round trips overlap; the ballots keep the flattened order
+        int col = 0;
+        int2 w = cw[0];
+        int cend = w.x, base = w.y;
+#pragma unroll 1
+        for (int k0 = 0; k0 < maxtotal; k0 += 2 * LPP) {
+            const int ka = k0 + sl, kb = ka + LPP;
+            const bool acta = ka < total, actb = kb < total;
+            int ja = 0, jb = 0;
+            if (acta) {
+                while (ka >= cend) {
+                    col++;
+                    w = cw[col];
+                    cend = w.x;
+                    base = w.y;
+                }
+                ja = base + ka;
             }
+            if (actb) {
+                while (kb >= cend) {
+                    col++;
+                    w = cw[col];
+                    cend = w.x;
+                    base = w.y;
+                }
+                jb = base + kb;
+            }
+            float4 Pa = make_float4(0.f, 0.f, 0.f, 0.f), Pb = Pa;
+            float2 ta = make_float2(0.f, 0.f), tb = ta;
+            if (acta) {
+                Pa = rP[ja];
+                if (COND == MFREE_COND_PSE) ta = reinterpret_cast<const float2 *>(rC + ja)[1];
+            }
+            if (actb) {
+                Pb = rP[jb];
+                if (COND == MFREE_COND_PSE) tb = reinterpret_cast<const float2 *>(rC + jb)[1];
+            }
+            bool insa = false, insb = false;
+            if (acta) {
+                const float r2 = dist2_rn(I.x - Pa.x, I.y - Pa.y, I.z - Pa.z);
+                insa = !(r2 >= four_h2) && (r2 > 9.99999994e-9f);
+                if (COND == MFREE_COND_PSE) {
+                    float e2;
+                    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e2) : "f"(pse_k * r2));
+                    pse = fmaf((ta.x - I.T) * ta.y, e2, pse);
+                }
+            }
+            if (actb) {
+                const float r2 = dist2_rn(I.x - Pb.x, I.y - Pb.y, I.z - Pb.z);
+                insb = !(r2 >= four_h2) && (r2 > 9.99999994e-9f);
+                if (COND == MFREE_COND_PSE) {
+                    float e2;
+                    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e2) : "f"(pse_k * r2));
+                    pse = fmaf((tb.x - I.T) * tb.y, e2, pse);
+                }
+            }
+            const unsigned ma = __ballot_sync(0xffffffffu, insa) & gmask;
+            const unsigned mb = __ballot_sync(0xffffffffu, insb) & gmask;
+            const int qa = qn + __popc(ma & lt_mask), qb = qn + __popc(ma) + __popc(mb & lt_mask);
+            if (insa && qa < QCAP_T) qq[qa] = ja;
+            if (insb && qb < QCAP_T) qq[qb] = jb;
+            qn += __popc(ma) + __popc(mb);
         }
-        const unsigned m = __ballot_sync(0xffffffffu, ins) & gmask;
-        if (ins) {
-            const int pos = qn + __popc(m & lt_mask);
-            if (pos < QCAP_T) qq[pos] = j;
-        }
-        qn += __popc(m);
-    });
+    }
     if (COND == MFREE_COND_PSE) {  // the PSE sum waits in the target's result slot
 #pragma unroll
         for (int o = LPP / 2; o >= 1; o >>= 1) pse += __shfl_xor_sync(0xffffffffu, pse, o);
@@ -570,13 +615,13 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
         float Bm[6];  // xx, yy, zz, xy, xz, yz
 #pragma unroll
         for (int k = 0; k < 6; k++) Bm[k] = 0.f;
-        auto bterm = [&](int j) {
-            const float4 Pj = rP[j];
+        // one neighbour's term: B += sv d (x) d with sv = -V_j dfac
+        auto bvals = [&](const float4 Pj, float vj) {
             if (I.tool == 1.f || Pj.w == 1.f) return;
             const float dx = I.x - Pj.x, dy = I.y - Pj.y, dz = I.z - Pj.z;
             float w, dfac;
             spline(dist2_rn(dx, dy, dz), I.h1, I.fac, w, dfac);
-            const float sv = -rC[j].w * dfac;  // -V_j dfac: B += sv d (x) d
+            const float sv = -vj * dfac;
             const float tx = sv * dx, ty = sv * dy, tz = sv * dz;
             Bm[0] = fmaf(tx, dx, Bm[0]);
             Bm[1] = fmaf(ty, dy, Bm[1]);
@@ -585,9 +630,21 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
             Bm[4] = fmaf(tx, dz, Bm[4]);
             Bm[5] = fmaf(ty, dz, Bm[5]);
         };
-        for (int q0 = 0; q0 < maxq; q0 += LPP) {
-            const int q = q0 + sl;
-            if (q < qv) bterm(qq[q]);
+        auto bterm = [&](int j) { bvals(rP[j], rC[j].w); };
+        // two queue entries per lane and iteration (q and q + LPP): both loads
+        // before either term, so the shared-memory round trips overlap; each
+        // lane still adds its terms in queue order
+#pragma unroll 1
+        for (int q0 = 0; q0 < maxq; q0 += 2 * LPP) {
+            const int qa = q0 + sl, qb = qa + LPP;
+            const bool a = qa < qv, b = qb < qv;
+            const int ja = a ? qq[qa] : 0, jb = b ? qq[qb] : 0;
+            float4 Pa = make_float4(0.f, 0.f, 0.f, 0.f), Pb = Pa;
+            float va = 0.f, vb = 0.f;
+            if (a) { Pa = rP[ja]; va = rC[ja].w; }
+            if (b) { Pb = rP[jb]; vb = rC[jb].w; }
+            if (a) bvals(Pa, va);
+            if (b) bvals(Pb, vb);
         }
         if (overflow) for_overflow(bterm);
 #pragma unroll
