@@ -224,6 +224,33 @@ def hbm_roofline(rate: float, sc) -> dict:
             "note": "the step is bound by the pair kernel's FP32 pipe, not by HBM"}
 
 
+def kernel_hbm(sc, n_act: int, step_ms: dict) -> dict:
+    """HBM roofline of the memory-bound kernels of the step, from their
+    CUDA-event times: algorithmic bytes per launch (each array element the
+    kernel must read or write, once) / time, against the measured copy
+    bandwidth."""
+    prec = 32 if sc.options.get("precision") else 0
+    blank = sc.blank_vmax > 0
+    # kb_gather_predict: perm 4 + state 176 (+ low parts) + key 4 read; state 176 (+ low parts)
+    # + sorted key 4 + neighbour records 96 written
+    gather = 4 + 176 + prec + 4 + 176 + prec + 4 + 96
+    # kb_hash: pos + blank flag 32 (+ vel 16 + rates 64 with blanking) read, key 4 written
+    hsh = 32 + (80 if blank else 0) + 4
+    peak = 6650.0
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        pass
+    out = {}
+    for k, b in (("gather_predict", gather), ("hash", hsh)):
+        ms = step_ms.get(k, 0.0)
+        if ms > 0:
+            gbs = sc.n * b / (ms * 1e-3) / 1e9
+            out[k] = {"bytes_per_particle": b, "ms": ms, "achieved_gbs": gbs, "frac": gbs / peak}
+    return out
+
+
 # -------------------------------------------------------------- oracle ----
 def cpu_model() -> str:
     """The host CPU's model name (/proc/cpuinfo), for the baseline's record."""
@@ -386,7 +413,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
             "kernel_ms_per_step": step_ms_dev,
             "clocks": clk.summary(),
             "counters": counters,
-            "hbm": hbm_roofline(value, sc)}
+            "hbm": hbm_roofline(value, sc),
+            "hbm_kernels": kernel_hbm(sc, n_act, step_ms_dev)}
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.workload)
     if world == 1 and not args.no_extras:

@@ -10,11 +10,13 @@
 // A step is 11 kernels on one stream with no host synchronisation (N lives on
 // the device), so it can also be captured once into a CUDA graph and replayed.
 #include <climits>
+#include <cstdint>
 #include <cstddef>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -37,10 +39,40 @@ void mfree::set_last_error(const std::string &msg) { g_err = msg; }
 namespace mfree {
 namespace host {
 
+// Context memory comes from one stream-ordered memory pool per device that
+// keeps what is freed (unlimited release threshold): contexts created and
+// destroyed one after another -- served requests, the autotuner's copies, a
+// caller's repeated jobs -- reuse it without a new cudaMalloc, and freeing
+// needs no device-wide synchronisation.  The pool is created on first use on
+// each device.
+cudaMemPool_t context_pool(int dev) {
+    static std::mutex m;
+    static std::vector<cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(m);
+    if (int(pools.size()) <= dev) pools.resize(size_t(dev) + 1, nullptr);
+    if (!pools[dev]) {
+        cudaMemPoolProps pr{};
+        pr.allocType = cudaMemAllocationTypePinned;
+        pr.location.type = cudaMemLocationTypeDevice;
+        pr.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &pr) != cudaSuccess) return nullptr;
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[dev] = pool;
+    }
+    return pools[dev];
+}
+
 template <class T> int dalloc(mfree_ctx *c, T **p, size_t n, std::vector<void *> &list) {
     void *q = nullptr;
-    cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
-    if (e != cudaSuccess) return fail(MFREE_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    cudaMemPool_t pool = context_pool(c->device);
+    if (!pool) return fail(MFREE_ERR_CUDA, "cudaMemPoolCreate failed");
+    cudaError_t e = cudaMallocFromPoolAsync(&q, std::max<size_t>(n, 1) * sizeof(T), pool, c->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(MFREE_ERR_OOM, std::string("cudaMallocFromPoolAsync: ") + cudaGetErrorString(e));
+    }
     list.push_back(q);
     *p = (T *)q;
     (&list == &c->scratch_allocs ? c->scratch_bytes : c->bytes) += std::max<size_t>(n, 1) * sizeof(T);
@@ -49,8 +81,9 @@ template <class T> int dalloc(mfree_ctx *c, T **p, size_t n, std::vector<void *>
 
 size_t device_bytes(const mfree_ctx *c) { return c->bytes + c->scratch_bytes; }
 
-void free_list(std::vector<void *> &l) {
-    for (void *p : l) cudaFree(p);
+// stream-ordered: the memory returns to the pool once the stream's earlier work is done
+void free_list(std::vector<void *> &l, cudaStream_t s) {
+    for (void *p : l) cudaFreeAsync(p, s);
     l.clear();
 }
 
@@ -177,7 +210,7 @@ int ensure_scratch(mfree_ctx *c) {
     // an unlocked grid changes its cell count every step: its scratch holds max_cell cells
     const long cells = c->grid_adaptive ? c->max_cell : c->num_cell;
     if (c->scratch_cells == size_t(cells) && !c->scratch_allocs.empty()) return MFREE_OK;
-    free_list(c->scratch_allocs);
+    free_list(c->scratch_allocs, c->stream);
     c->scratch_bytes = 0;
     auto &L = c->scratch_allocs;
     int st;
@@ -406,7 +439,7 @@ int alloc_ctx(int n, cudaStream_t stream, std::unique_ptr<mfree_ctx> &out) {
     c->opt.max_secant_iter = 100;
     auto &L = c->allocs;
     auto bail = [&](int st) {
-        free_list(c->allocs);
+        free_list(c->allocs, c->stream);
         if (c->own_stream) cudaStreamDestroy(c->stream);
         return st;
     };
@@ -572,8 +605,8 @@ int mfree_destroy(mfree_ctx *c) {
         if (t->d_tri) cudaFree(t->d_tri);
         if (t->d_cells) cudaFree(t->d_cells);
     }
-    free_list(c->scratch_allocs);
-    free_list(c->allocs);
+    free_list(c->scratch_allocs, c->stream);
+    free_list(c->allocs, c->stream);
     for (auto &t : c->tev) {
         cudaEventDestroy(t.second.first);
         cudaEventDestroy(t.second.second);
