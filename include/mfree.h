@@ -153,6 +153,8 @@ typedef struct {
     int64_t full_stencil_steps; /* steps whose pair loop fell back to the full 5x5x5
                                    stencil because a particle moved too far in the
                                    predictor (variants without PSE; see full_stencil) */
+    int64_t bounds_errors;      /* bounds-checked library only: data-derived indices
+                                   that fell outside their array (always 0 otherwise) */
 } mfree_counters;
 
 typedef struct mfree_ctx mfree_ctx;
@@ -278,6 +280,9 @@ int mfree_get_cells(mfree_ctx *ctx, int *cell_start, int *cell_end);
 int mfree_get_grid(const mfree_ctx *ctx, long *nx, long *ny, long *nz,
                    float *bbmin3, float *dx);
 int mfree_get_counters(mfree_ctx *ctx, mfree_counters *out);
+/* 1 in the bounds-checked build of the library (libmfree_checked.so, a debug
+ * stand-in for a memory checker; no counterpart in the reference), else 0 */
+int mfree_bounds_checked(void);
 /* Failure injection for tests (no reference counterpart).  MFREE_FAULT_STAGING_WAIT
  * raises the byte count the pair kernel's staging waits expect, so every wait
  * runs out after its bound (~0.5 s), the kernel counts it and leaves, and the

@@ -45,6 +45,7 @@ EXPORTS = [
     "mfree_batch_timer_stop", "mfree_device_bytes", "mfree_scene_bytes", "mfree_write_vtk", "mfree_output_wait",
     "mfree_write_vtk_tools", "mfree_write_vtk_blanking", "mfree_append_force_log", "mfree_export_state",
     "mfree_import_state", "mfree_inject_fault", "mfree_get_array", "mfree_set_array", "mfree_array_device_ptr",
+    "mfree_bounds_checked",
 ]
 ARRAYS = ["POS_H", "VEL_RHO", "S_A", "S_B", "POS_T", "VEL_T", "S_T_A", "S_T_B", "FC", "FT", "VEL_BC", "LO", "LO_B"]
 ERR_ARG = -1
@@ -84,7 +85,8 @@ class Options(C.Structure):
 
 class Counters(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("steps", "secant_failures", "out_of_grid", "contact_search_cap",
-                                         "nan_blanked", "staging_timeouts", "full_stencil_steps")]
+                                         "nan_blanked", "staging_timeouts", "full_stencil_steps",
+                                         "bounds_errors")]
 
 
 _lib = None

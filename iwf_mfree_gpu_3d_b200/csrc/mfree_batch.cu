@@ -160,6 +160,7 @@ int build_table(mfree_batch *b, int record_every) {
 // the kernels of one batch step (record_mode as kb_clock; 2 = every
 // Params::record_every steps of each scene's own step index)
 int enqueue_batch_step(mfree_batch *b, int record_mode) {
+    const TraceRange range("mfree_batch_step");
     const BatchTable &T = b->T;
     cudaStream_t s = b->stream;
     const int n = T.nscenes;

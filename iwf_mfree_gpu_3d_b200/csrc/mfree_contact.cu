@@ -138,6 +138,7 @@ __device__ void closest_by_shells(const ToolDev &T, const ToolClock &B, float t,
     cp = qp;
     nrm = v3(0.f, 0.f, 0.f);
     int box = (ix * T.ny + iy) * T.nz + iz;
+    if (T.cells[box + 1] > T.cells[box] && !bounds_ok(clk, T.cells[box + 1] - 1, T.num_tris)) return;
     bool empty_so_far = T.cells[box] == T.cells[box + 1];
     for (int k = T.cells[box]; k < T.cells[box + 1]; k++) {
         V3 c, n;
@@ -158,6 +159,7 @@ __device__ void closest_by_shells(const ToolDev &T, const ToolClock &B, float t,
                     bool on = a == li || a == hi - 1 || b == lj || b == hj - 1 || c == lk || c == hk - 1;
                     if (!on) continue;
                     const int bx = (a * T.ny + b) * T.nz + c;
+                    if (T.cells[bx + 1] > T.cells[bx] && !bounds_ok(clk, T.cells[bx + 1] - 1, T.num_tris)) continue;
                     for (int k = T.cells[bx]; k < T.cells[bx + 1]; k++) {
                         empty_so_far = false;
                         V3 cc, n;

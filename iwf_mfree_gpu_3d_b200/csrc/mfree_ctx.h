@@ -7,6 +7,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "mfree.h"
 #include "mfree_kernels.cuh"
 #include "mfree_tool.h"
@@ -29,6 +31,19 @@ int fail(int code, const std::string &msg);
 
 namespace mfree {
 namespace host {
+
+// NVTX range around a host-side call or kernel launch, for timeline tools
+// (Nsight Systems); with no tool attached a push/pop costs a few nanoseconds
+struct TraceRange {
+    explicit TraceRange(const char *name) { nvtxRangePushA(name); }
+    ~TraceRange() { nvtxRangePop(); }
+    TraceRange(const TraceRange &) = delete;
+    TraceRange &operator=(const TraceRange &) = delete;
+};
+// the step's kernels in launch order (the ids of mfree_get_kernel_times)
+constexpr const char *KERNEL_TRACE_NAMES[MFREE_NUM_KERNELS] = {
+    "kb_clock", "kb_hash", "kb_scan_reduce", "kb_scan_top", "kb_scan_down", "kb_scatter",
+    "kb_cell_fixup", "kb_gather_predict", "kb_interact", "kb_finalize", "kb_force_final"};
 
 struct DevTool {
     HostTool host;

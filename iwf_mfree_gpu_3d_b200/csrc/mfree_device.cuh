@@ -56,7 +56,23 @@ struct DevClock {
     ToolClock tool[MAX_TOOLS];
     // device-detected conditions (mfree_counters)
     unsigned long long secant_failures, out_of_grid, contact_cap, nan_blanked, full_stencil_steps;
+    unsigned long long bounds_errors;  // bounds-checked builds: indices from data that fell outside their array
 };
+
+// Bounds-checked build (-DMFREE_BOUNDS_CHECK, libmfree_checked.so): every
+// index computed from data at the places below is tested against its array;
+// one outside is counted in the scene's clock and the access is skipped or
+// redirected to element 0, so a wrong index shows as a count, not a fault.
+// In the normal build the test is constant true and compiles away.
+#ifdef MFREE_BOUNDS_CHECK
+__device__ __forceinline__ bool bounds_ok(DevClock *clk, long long idx, long long lim) {
+    if (idx >= 0 && idx < lim) return true;
+    if (clk) atomicAdd(&clk->bounds_errors, 1ull);
+    return false;
+}
+#else
+__device__ __forceinline__ constexpr bool bounds_ok(DevClock *, long long, long long) { return true; }
+#endif
 
 struct ToolDev {
     // boxed (hashed) or all (exhaustive) triangles, SoA of float4 (x, y, z, -)

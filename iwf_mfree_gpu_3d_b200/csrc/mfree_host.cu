@@ -355,6 +355,7 @@ int enqueue_step(mfree_ctx *c, int record_mode, int record_every, bool timed = f
             e1 = pooled_event(c);
             cudaEventRecord(e0, s);
         }
+        const TraceRange range(KERNEL_TRACE_NAMES[id]);
         launch();
         if (timed) {
             cudaEventRecord(e1, s);
@@ -932,6 +933,7 @@ int adapt_grid(mfree_ctx *c) {
 
 int mfree_step(mfree_ctx *c, int record_forces) {
     if (!c) return fail(MFREE_ERR_ARG, "null context");
+    const TraceRange range("mfree_step");
     if (c->owner) return fail(MFREE_ERR_ARG, "mfree_step: the context belongs to a batch (mfree_batch_step steps it)");
     int st = ready(c);
     if (st) return st;
@@ -948,6 +950,7 @@ int mfree_step(mfree_ctx *c, int record_forces) {
 
 int mfree_advance(mfree_ctx *c, int nsteps, int record_every, int use_graph) {
     if (!c || nsteps < 0) return fail(MFREE_ERR_ARG, "bad arguments");
+    const TraceRange range("mfree_advance");
     if (c->owner) return fail(MFREE_ERR_ARG, "mfree_advance: the context belongs to a batch (mfree_batch_step steps it)");
     int st = ready(c);
     if (st) return st;
@@ -1090,7 +1093,16 @@ int mfree_get_counters(mfree_ctx *c, mfree_counters *o) {
     o->nan_blanked = int64_t(h.nan_blanked);
     o->staging_timeouts = int64_t(h.staging_timeouts);
     o->full_stencil_steps = int64_t(h.full_stencil_steps);
+    o->bounds_errors = int64_t(h.bounds_errors);
     return MFREE_OK;
+}
+
+int mfree_bounds_checked(void) {
+#ifdef MFREE_BOUNDS_CHECK
+    return 1;
+#else
+    return 0;
+#endif
 }
 
 int mfree_field_width(int f) {

@@ -408,6 +408,7 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
         if (STAGED) {
             const int lc = (gi - X0 + 2) * HY + (gj - Y0 + 2);
             si = sm.hoff[lc] + (i - sm.hstart[lc]);
+            if (!bounds_ok(a.clk, si, rstride)) si = 0;
         }
         const float4 Pi = rP[si], Vi = rV[si], Ai = rA[si], Bi = rB[si], Ri = rR[si], Ci = rC[si];
         I.x = Pi.x; I.y = Pi.y; I.z = Pi.z; I.tool = Pi.w;
@@ -509,7 +510,9 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
                     base = w.y;
                 }
             }
-            fn(base + k, act);
+            int j = base + k;
+            if (act && !bounds_ok(a.clk, j, rstride)) j = 0;
+            fn(j, act);
         }
     };
     // ---- pass A: support test, PSE, queue
@@ -536,6 +539,7 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
                     base = w.y;
                 }
                 ja = base + ka;
+                if (!bounds_ok(a.clk, ja, rstride)) ja = 0;
             }
             if (actb) {
                 while (kb >= cend) {
@@ -545,6 +549,7 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
                     base = w.y;
                 }
                 jb = base + kb;
+                if (!bounds_ok(a.clk, jb, rstride)) jb = 0;
             }
             float4 Pa = make_float4(0.f, 0.f, 0.f, 0.f), Pb = Pa;
             float2 ta = make_float2(0.f, 0.f), tb = ta;
@@ -926,7 +931,8 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
                 const int tg = t0 + tt;
                 int c = 0;
                 while (c < NTC - 1 && sm.tpref[c + 1] <= tg) c++;
-                const int i = sm.tstart[c] + (tg - sm.tpref[c]);
+                int i = sm.tstart[c] + (tg - sm.tpref[c]);
+                if (!bounds_ok(a.clk, i, a.p.n_init)) i = 0;
                 sm.tgt[tt] = i;
                 // its cell: the z row of its column whose range holds i (the
                 // rows up to the tile's last target cell are in the table)

@@ -261,9 +261,11 @@ __device__ __forceinline__ void scatter_body(const StepArgs &a, int bid) {
     if (i >= P.n_init) return;
     if (!blank) {
         int old = atomicSub(&a.s.count[key], 1);  // leaves count[] zero for the next step
-        a.s.perm[a.s.first[key] + old - 1] = i;
+        const int d = a.s.first[key] + old - 1;
+        if (bounds_ok(a.clk, d, P.n_init)) a.s.perm[d] = i;
     } else {
-        a.s.perm[N + a.s.blank_block[bid] + rank] = i;
+        const int d = N + a.s.blank_block[bid] + rank;
+        if (bounds_ok(a.clk, d, P.n_init)) a.s.perm[d] = i;
     }
 }
 __global__ void __launch_bounds__(HASH_BLOCK) k_scatter(StepArgs a) { scatter_body(a, blockIdx.x); }
@@ -277,6 +279,7 @@ __device__ __forceinline__ void cell_fixup_body(const StepArgs &a, int bid) {
     if (c >= a.p.num_cell) return;
     const int s = a.s.first[c], e = a.s.first[c + 1];
     if (e - s < 2) return;
+    if (!bounds_ok(a.clk, s, a.p.n_init) || !bounds_ok(a.clk, e - 1, a.p.n_init)) return;
     int *p = a.s.perm;
     for (int k = s + 1; k < e; k++) {
         int v = p[k];
