@@ -29,7 +29,8 @@ At N = 1 the line also carries the two systems forms, measured live:
     150 GB budget, with p50/p99 latency (arrival to result) and throughput;
     rate, duration, sizes and step counts are scaled down so the run takes
     seconds (the scaling is stated in the line).
---no-extras skips both.
+  * "precision_form" (1M workload): the same step in the precision form.
+--no-extras skips these.
 """
 from __future__ import annotations
 
@@ -417,6 +418,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
             "hbm_kernels": kernel_hbm(sc, n_act, step_ms_dev)}
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.workload)
+    if world == 1 and not args.no_extras and args.workload == "1m":
+        line["precision_form"] = run_precision_form(sc, args, opts)
     if world == 1 and not args.no_extras:
         line["batched"] = run_batched(args)
         line["serving"] = run_serve(args, tuple(line["batched"]["tiling"]))
@@ -424,6 +427,23 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
 
 
 # ------------------------------------------------------ systems forms -----
+def run_precision_form(sc, args, opts) -> dict:
+    """The 1M configuration's second run: the precision form (FP32 bulk,
+    compensated hi/lo positions and velocities), timed like the main line."""
+    from iwf_mfree_gpu_3d_b200 import api
+    sim = api.Simulation.from_scene(sc, precision=1, **opts)
+    sim.advance(max(args.warmup, 3), use_graph=True)
+    sim.sync()
+    sim.timer_start()
+    sim.advance(args.steps, use_graph=True)
+    ms = sim.timer_stop()
+    sim.close()
+    return {"metric": "particle-steps/s", "value": sc.n * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps,
+            "dtype": "f32 + compensated hi/lo positions and velocities",
+            "timing": "CUDA events around K graph replays, as the main line",
+            "error_vs_fp64": "per-field relative L2 at step 100: tests/test_gpu_parity.py "
+                             "test_100_steps_against_fp64_oracle_full_size_1m_plain_and_precision"}
+
 def run_batched(args) -> dict:
     """Mixed-size scenes stepped together against the plain path scene by scene."""
     from iwf_mfree_gpu_3d_b200 import api, scenes
