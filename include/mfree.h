@@ -280,6 +280,15 @@ int mfree_get_cells(mfree_ctx *ctx, int *cell_start, int *cell_end);
 int mfree_get_grid(const mfree_ctx *ctx, long *nx, long *ny, long *nz,
                    float *bbmin3, float *dx);
 int mfree_get_counters(mfree_ctx *ctx, mfree_counters *out);
+/* FP64 reductions over the active workpiece particles of the current state
+ * (no counterpart in the reference, which steps with a fixed dt and reports
+ * no energies): out[0] kinetic energy sum m|v|^2/2, out[1] deviatoric elastic
+ * energy sum (m/rho) S:S/(4G), out[2] volumetric elastic energy sum
+ * (m/rho) p^2/(2K) with p = c0^2 (rho - rho0), out[3] thermal energy
+ * sum m cp (T - T_init), out[4] the CFL time-step bound min h/(c + |v|) with
+ * c = sqrt(K/rho) (multiply by the CFL number).  Computed in double on the
+ * device in a fixed order (the same bits on every call for the same state). */
+int mfree_get_energies(mfree_ctx *ctx, double out[5]);
 /* 1 in the bounds-checked build of the library (libmfree_checked.so, a debug
  * stand-in for a memory checker; no counterpart in the reference), else 0 */
 int mfree_bounds_checked(void);

@@ -45,7 +45,7 @@ EXPORTS = [
     "mfree_batch_timer_stop", "mfree_device_bytes", "mfree_scene_bytes", "mfree_write_vtk", "mfree_output_wait",
     "mfree_write_vtk_tools", "mfree_write_vtk_blanking", "mfree_append_force_log", "mfree_export_state",
     "mfree_import_state", "mfree_inject_fault", "mfree_get_array", "mfree_set_array", "mfree_array_device_ptr",
-    "mfree_bounds_checked",
+    "mfree_bounds_checked", "mfree_get_energies",
 ]
 ARRAYS = ["POS_H", "VEL_RHO", "S_A", "S_B", "POS_T", "VEL_T", "S_T_A", "S_T_B", "FC", "FT", "VEL_BC", "LO", "LO_B"]
 ERR_ARG = -1
@@ -117,6 +117,7 @@ def lib(path: str = LIB_PATH):
     L.mfree_set_grid_velocity.argtypes = [P, fp]
     L.mfree_set_grid_adaptive.argtypes = [P, C.c_long]
     L.mfree_get_array.argtypes = [P, I, fp]
+    L.mfree_get_energies.argtypes = [P, C.POINTER(C.c_double)]
     L.mfree_set_array.argtypes = [P, I, fp]
     L.mfree_array_device_ptr.argtypes = [P, I, C.POINTER(P)]
     L.mfree_set_blanking.argtypes = [P, fp, fp, fp, F]
@@ -425,6 +426,13 @@ class Simulation:
         if a.size != 4 * self.n_init:
             raise ValueError(f"set_array({name!r}): {4 * self.n_init} floats expected")
         _check(self.L.mfree_set_array(self.h, ARRAYS.index(name), a.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def energies(self) -> dict:
+        """FP64 device reductions: kinetic, deviatoric and volumetric elastic, thermal energy and the CFL bound."""
+        out = (C.c_double * 5)()
+        _check(self.L.mfree_get_energies(self.h, out))
+        return dict(kinetic=out[0], elastic_deviatoric=out[1], elastic_volumetric=out[2], thermal=out[3],
+                    cfl_dt=out[4])
 
     def array_device_ptr(self, name: str) -> int:
         p = C.c_void_p()

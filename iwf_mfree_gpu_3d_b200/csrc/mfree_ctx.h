@@ -78,6 +78,7 @@ struct mfree_ctx {
     bool grid_adaptive = false;  // unlocked grid: box and cell edge from the particles every step
     long max_cell = 0;           // its cell limit (the scratch is sized for it)
     int *d_bbox = nullptr, *h_bbox = nullptr;  // its bounding-box reduction (device, page-locked host)
+    double *d_energy = nullptr;  // mfree_get_energies: results, then per-block partials
     bool blank_set = false;
     float b_min[3], b_max[3], b_vel[3] = {0, 0, 0}, b_vmax = 0.f;
     float dt = 0.f, t = 0.f;

@@ -1097,6 +1097,86 @@ int mfree_get_counters(mfree_ctx *c, mfree_counters *o) {
     return MFREE_OK;
 }
 
+// FP64 energy and CFL reductions: per-block partials in double, then one
+// block sums them in a fixed order (deterministic)
+constexpr int ENERGY_BLOCK = 256, ENERGY_VALUES = 5;
+__global__ void __launch_bounds__(ENERGY_BLOCK) k_energy_partial(State S, const DevClock *clk, int n_init, int stepped,
+                                                                 float mass,
+                                                                 float K, float G, float rho0, float c0sq, float cp,
+                                                                 float T0, double *part) {
+    __shared__ double red[ENERGY_VALUES][ENERGY_BLOCK / 32];
+    const int n = stepped ? min(clk->n_active, n_init) : n_init;  // active particles lead the sorted order
+    const int i = blockIdx.x * ENERGY_BLOCK + threadIdx.x;
+    double v[ENERGY_VALUES] = {0.0, 0.0, 0.0, 0.0, 1e300};
+    if (i < n) {
+        const float4 vel = S.vel4[i], sa = S.sa4[i], sb = S.sb4[i], pos = S.pos4[i];
+        if (S.fc4[i].w != 1.f && S.ft4[i].w != 1.f) {  // workpiece, not blanked
+            const double vx = vel.x, vy = vel.y, vz = vel.z, rho = vel.w;
+            const double v2 = vx * vx + vy * vy + vz * vz;
+            const double ss = double(sa.x) * sa.x + double(sa.y) * sa.y + double(sa.z) * sa.z +
+                              2.0 * (double(sa.w) * sa.w + double(sb.x) * sb.x + double(sb.y) * sb.y);
+            const double p = double(c0sq) * (rho - double(rho0));
+            const double vol = double(mass) / rho;
+            v[0] = 0.5 * double(mass) * v2;
+            v[1] = vol * ss / (4.0 * double(G));
+            v[2] = vol * p * p / (2.0 * double(K));
+            v[3] = double(mass) * double(cp) * (double(sb.z) - double(T0));
+            v[4] = double(pos.w) / (sqrt(double(K) / rho) + sqrt(v2));
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < ENERGY_VALUES; k++) {
+        double x = v[k];
+        for (int o = 16; o >= 1; o >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, x, o);
+            x = k < 4 ? x + y : fmin(x, y);
+        }
+        if (lane == 0) red[k][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < ENERGY_VALUES) {
+        const int k = threadIdx.x;
+        double x = red[k][0];
+        for (int w = 1; w < ENERGY_BLOCK / 32; w++) x = k < 4 ? x + red[k][w] : fmin(x, red[k][w]);
+        part[size_t(blockIdx.x) * ENERGY_VALUES + k] = x;
+    }
+}
+__global__ void __launch_bounds__(ENERGY_VALUES * 32) k_energy_final(const double *part, int nb, double *out) {
+    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double x = k < 4 ? 0.0 : 1e300;
+    for (int b = lane; b < nb; b += 32) {
+        const double y = part[size_t(b) * ENERGY_VALUES + k];
+        x = k < 4 ? x + y : fmin(x, y);
+    }
+    for (int o = 16; o >= 1; o >>= 1) {
+        const double y = __shfl_xor_sync(0xffffffffu, x, o);
+        x = k < 4 ? x + y : fmin(x, y);
+    }
+    if (lane == 0) out[k] = x;
+}
+
+int mfree_get_energies(mfree_ctx *c, double out[5]) {
+    if (!c || !out) return fail(MFREE_ERR_ARG, "null argument");
+    if (!(c->phys.G > 0.f) || !(c->phys.K > 0.f) || !(c->phys.rho0 > 0.f))
+        return fail(MFREE_ERR_ARG, "mfree_get_energies: physics constants not set");
+    const int nb = std::max(1, (c->n_init + ENERGY_BLOCK - 1) / ENERGY_BLOCK);
+    if (!c->d_energy) {
+        int st = dalloc(c, &c->d_energy, size_t(nb) * ENERGY_VALUES + ENERGY_VALUES, c->allocs);
+        if (st) return st;
+    }
+    const float c0 = std::sqrt(c->phys.K / c->phys.rho0);
+    k_energy_partial<<<nb, ENERGY_BLOCK, 0, c->stream>>>(c->st[c->cur], c->d_clk, c->n_init, c->steps > 0 ? 1 : 0,
+                                                          c->phys.mass,
+                                                          c->phys.K, c->phys.G, c->phys.rho0, c0 * c0, c->twp.cp,
+                                                          c->twp.T_init, c->d_energy + ENERGY_VALUES);
+    k_energy_final<<<1, ENERGY_VALUES * 32, 0, c->stream>>>(c->d_energy + ENERGY_VALUES, nb, c->d_energy);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(out, c->d_energy, sizeof(double) * ENERGY_VALUES, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return MFREE_OK;
+}
+
 int mfree_bounds_checked(void) {
 #ifdef MFREE_BOUNDS_CHECK
     return 1;

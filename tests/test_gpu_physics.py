@@ -259,3 +259,37 @@ def test_compact_arrays_match_the_reference_layout_fields():
         np.testing.assert_array_equal(a.get(name), b.get(name), err_msg=name)
     for s in (sim, a, b):
         s.close()
+
+
+def test_fp64_energy_and_cfl_reductions_match_the_fields():
+    """mfree_get_energies: FP64 device reductions of the current state against
+    the same sums in numpy FP64 from the fields; repeated calls give the same
+    bits."""
+    sc = scenes.small_scene()
+    sim = api.Simulation.from_scene(sc)
+    sim.advance(20, use_graph=True)
+    e1, e2 = sim.energies(), sim.energies()
+    assert e1 == e2
+    n_act = sim.counts()[0]
+    vel = sim.get("VEL")[:n_act, :3].astype(np.float64)
+    rho = sim.get("RHO")[:n_act].astype(np.float64)
+    S = sim.get("S").reshape(-1, 9)[:n_act].astype(np.float64)
+    T = sim.get("T")[:n_act].astype(np.float64)
+    h = sim.get("H")[:n_act].astype(np.float64)
+    wp = (sim.get("TOOL_PARTICLE")[:n_act] != 1.0) & (sim.get("BLANKED")[:n_act] != 1.0)
+    m, K, G, rho0 = (np.float64(np.float32(sc.phys[k])) for k in ("mass", "K", "G", "rho0"))
+    c0sq = np.float64(np.float32(np.sqrt(np.float32(sc.phys["K"]) / np.float32(sc.phys["rho0"]))) ** 2)
+    v2 = (vel ** 2).sum(axis=1)
+    ss = (S ** 2).sum(axis=1)
+    p = c0sq * (rho - rho0)
+    terms = dict(kinetic=(0.5 * m * v2)[wp],
+                 elastic_deviatoric=((m / rho) * ss / (4 * G))[wp],
+                 elastic_volumetric=((m / rho) * p * p / (2 * K))[wp],
+                 thermal=(m * np.float64(np.float32(sc.trml_wp["cp"])) *
+                          (T - np.float64(np.float32(sc.trml_wp["T_init"]))))[wp])
+    for k, t in terms.items():  # sums: within 1e-9 of the sum of magnitudes (summation order)
+        assert abs(e1[k] - t.sum()) <= 1e-9 * np.abs(t).sum() + 1e-300, (k, e1[k], t.sum())
+    cfl = (h / (np.sqrt(K / rho) + np.sqrt(v2)))[wp].min()
+    assert abs(e1["cfl_dt"] - cfl) <= 1e-12 * cfl, (e1["cfl_dt"], cfl)
+    assert e1["kinetic"] > 0 and e1["elastic_deviatoric"] > 0 and e1["cfl_dt"] > 0
+    sim.close()
