@@ -286,8 +286,10 @@ int mfree_get_counters(mfree_ctx *ctx, mfree_counters *out);
  * energy sum (m/rho) S:S/(4G), out[2] volumetric elastic energy sum
  * (m/rho) p^2/(2K) with p = c0^2 (rho - rho0), out[3] thermal energy
  * sum m cp (T - T_init), out[4] the CFL time-step bound min h/(c + |v|) with
- * c = sqrt(K/rho) (multiply by the CFL number).  Computed in double on the
- * device in a fixed order (the same bits on every call for the same state). */
+ * c = sqrt(K/rho) (multiply by the CFL number).  In the precision form
+ * (options.precision = 1) the velocity is hi + lo of the compensated
+ * accumulation.  Computed in double on the device in a fixed order (the same
+ * bits on every call for the same state). */
 int mfree_get_energies(mfree_ctx *ctx, double out[5]);
 /* 1 in the bounds-checked build of the library (libmfree_checked.so, a debug
  * stand-in for a memory checker; no counterpart in the reference), else 0 */
@@ -332,7 +334,10 @@ int mfree_set_device(int device);
  *   pos4:       device pointer, n float4 positions (w ignored)
  *   bbmin, dx, nx, ny, nz: the grid (mfree_get_grid)
  *   perm:       device pointer, n ints out: sorted position -> input index;
- *               positions outside the grid come last, in input order
+ *               positions outside the grid, and positions with a NaN or
+ *               infinite coordinate, come last, in input order (as in the
+ *               step's truncating hash, a coordinate less than one cell below
+ *               the grid's lower corner still falls in cell 0 of its axis)
  *   cell_first: device pointer, nx*ny*nz + 1 ints out: index of the first
  *               sorted position of each cell; cell_first[nx*ny*nz] = number of
  *               positions inside the grid
@@ -341,7 +346,9 @@ int mfree_set_device(int device);
  * else MFREE_ERR_ARG.  The array (about 3 MiB) is held on every GPU that loads
  * the library until the process exits.  The first call on a device looks up
  * the array's device address (cudaGetSymbolAddress); make that first call
- * before any stream capture.  All calls share the array and it keeps the last
+ * before any stream capture.  The address is kept for the life of the
+ * process: after cudaDeviceReset on a device, do not call this function on
+ * that device again.  All calls share the array and it keeps the last
  * call's contents (the counters are cleared at the start of each call): calls
  * that overlap on the GPU race. */
 #define MFREE_STATIC_MAX_PARTICLES 262144

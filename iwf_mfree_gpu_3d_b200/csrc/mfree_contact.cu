@@ -16,25 +16,22 @@
 //
 // One thread per particle; only particles inside a tool box do contact work
 // (the pair kernel's epilogue has already finished every other particle).
+#include "mfree_geom.h"
 #include "mfree_kernels.cuh"
 
 namespace mfree {
 
 namespace {
 
-struct V3 {
-    float x, y, z;
-};
+// vector algebra of the contact code on the shared float 3-vector
+using V3 = Vec3f;
 __device__ __forceinline__ V3 v3(float x, float y, float z) { return {x, y, z}; }
-__device__ __forceinline__ V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-__device__ __forceinline__ V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-__device__ __forceinline__ V3 operator*(float s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
-__device__ __forceinline__ bool operator==(V3 a, V3 b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
-__device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-__device__ __forceinline__ V3 cross(V3 a, V3 b) {
-    return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y};
-}
-__device__ __forceinline__ float len(V3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ V3 operator+(V3 a, V3 b) { return vadd(a, b); }
+__device__ __forceinline__ V3 operator-(V3 a, V3 b) { return vsub(a, b); }
+__device__ __forceinline__ V3 operator*(float s, V3 a) { return vscale(s, a); }
+__device__ __forceinline__ float dot(V3 a, V3 b) { return vdot(a, b); }
+__device__ __forceinline__ V3 cross(V3 a, V3 b) { return vcross(a, b); }
+__device__ __forceinline__ float len(V3 a) { return vlength(a); }
 __device__ __forceinline__ V3 ld(const float4 *p, int i) {
     float4 v = p[i];
     return {v.x, v.y, v.z};
@@ -46,37 +43,18 @@ __device__ __forceinline__ V3 vert(const ToolDev &T, const float4 *p, int i, flo
     return {v.x + T.vel[0] * t, v.y + T.vel[1] * t, v.z + T.vel[2] * t};
 }
 
-__device__ V3 closest_on_segment(V3 p1, V3 p2, V3 p) {
-    float dx = p1.x - p2.x, dy = p1.y - p2.y, dz = p1.z - p2.z;
-    float ns2 = dx * dx + dy * dy + dz * dz;
-    if (ns2 == 0.f) return p1;
-    float t = ((p2.x - p1.x) * (p.x - p1.x) + (p2.y - p1.y) * (p.y - p1.y) + (p2.z - p1.z) * (p.z - p1.z)) / ns2;
-    if (t > 1.f) return p2;
-    if (t < 0.f) return p1;
-    return (1.f - t) * p1 + t * p2;
-}
-
 // closest point on triangle k and the normal of the feature it lies on
-// (comp_closest_point, tool_3d_gpu.cu:141-212)
+// (comp_closest_point, tool_3d_gpu.cu:141-212; the geometry is shared with the
+// host setup in mfree_geom.h)
 __device__ void closest_point(const ToolDev &T, int k, float t, V3 qp, V3 &cp, V3 &np) {
-    V3 p1 = vert(T, T.p1, k, t), p2 = vert(T, T.p2, k, t), p3 = vert(T, T.p3, k, t);
-    V3 p1p2 = p2 - p1, p1p3 = p3 - p1, pp1 = p1 - qp;
-    float B = dot(p1p3, p1p2), E = dot(p1p2, p1p2), C = dot(p1p3, p1p3);
-    float det = B * B - E * C;
-    float A = dot(p1p3, pp1), D = dot(p1p2, pp1);
-    float t1 = (D * C - A * B) / det, t2 = (A * E - D * B) / det;
-    if (t1 < 0.f) {
-        cp = closest_on_segment(p1, p3, qp);
-        np = cp == p1 ? ld(T.np1, k) : (cp == p3 ? ld(T.np3, k) : ld(T.ne3, k));
-    } else if (t2 < 0.f) {
-        cp = closest_on_segment(p1, p2, qp);
-        np = cp == p1 ? ld(T.np1, k) : (cp == p2 ? ld(T.np2, k) : ld(T.ne1, k));
-    } else if (t1 + t2 > 1.f) {
-        cp = closest_on_segment(p2, p3, qp);
-        np = cp == p2 ? ld(T.np2, k) : (cp == p3 ? ld(T.np3, k) : ld(T.ne2, k));
-    } else {
-        cp = p1 + t1 * p1p2 + t2 * p1p3;
-        np = ld(T.n, k);
+    switch (closest_on_triangle(vert(T, T.p1, k, t), vert(T, T.p2, k, t), vert(T, T.p3, k, t), qp, cp)) {
+        case TF_V1: np = ld(T.np1, k); break;
+        case TF_V2: np = ld(T.np2, k); break;
+        case TF_V3: np = ld(T.np3, k); break;
+        case TF_E12: np = ld(T.ne1, k); break;
+        case TF_E23: np = ld(T.ne2, k); break;
+        case TF_E31: np = ld(T.ne3, k); break;
+        default: np = ld(T.n, k); break;
     }
 }
 

@@ -70,8 +70,16 @@ __device__ __forceinline__ bool bounds_ok(DevClock *clk, long long idx, long lon
     if (clk) atomicAdd(&clk->bounds_errors, 1ull);
     return false;
 }
+// a range [start, start + len) of an array of lim elements; len 0 is always
+// fine
+__device__ __forceinline__ bool range_ok(DevClock *clk, long long start, long long len, long long lim) {
+    if (len == 0 || (len > 0 && start >= 0 && start + len <= lim)) return true;
+    if (clk) atomicAdd(&clk->bounds_errors, 1ull);
+    return false;
+}
 #else
 __device__ __forceinline__ constexpr bool bounds_ok(DevClock *, long long, long long) { return true; }
+__device__ __forceinline__ constexpr bool range_ok(DevClock *, long long, long long, long long) { return true; }
 #endif
 
 struct ToolDev {

@@ -1101,7 +1101,7 @@ int mfree_get_counters(mfree_ctx *c, mfree_counters *o) {
 // block sums them in a fixed order (deterministic)
 constexpr int ENERGY_BLOCK = 256, ENERGY_VALUES = 5;
 __global__ void __launch_bounds__(ENERGY_BLOCK) k_energy_partial(State S, const DevClock *clk, int n_init, int stepped,
-                                                                 float mass,
+                                                                 int prec, float mass,
                                                                  float K, float G, float rho0, float c0sq, float cp,
                                                                  float T0, double *part) {
     __shared__ double red[ENERGY_VALUES][ENERGY_BLOCK / 32];
@@ -1111,7 +1111,14 @@ __global__ void __launch_bounds__(ENERGY_BLOCK) k_energy_partial(State S, const 
     if (i < n) {
         const float4 vel = S.vel4[i], sa = S.sa4[i], sb = S.sb4[i], pos = S.pos4[i];
         if (S.fc4[i].w != 1.f && S.ft4[i].w != 1.f) {  // workpiece, not blanked
-            const double vx = vel.x, vy = vel.y, vz = vel.z, rho = vel.w;
+            double vx = vel.x, vy = vel.y, vz = vel.z;
+            const double rho = vel.w;
+            if (prec) {  // the precision form: velocity = hi + lo of the compensated accumulation
+                const float4 lo = S.lo4[i], lob = S.lo4b[i];
+                vx += double(lo.w);
+                vy += double(lob.x);
+                vz += double(lob.y);
+            }
             const double v2 = vx * vx + vy * vy + vz * vz;
             const double ss = double(sa.x) * sa.x + double(sa.y) * sa.y + double(sa.z) * sa.z +
                               2.0 * (double(sa.w) * sa.w + double(sb.x) * sb.x + double(sb.y) * sb.y);
@@ -1167,7 +1174,7 @@ int mfree_get_energies(mfree_ctx *c, double out[5]) {
     }
     const float c0 = std::sqrt(c->phys.K / c->phys.rho0);
     k_energy_partial<<<nb, ENERGY_BLOCK, 0, c->stream>>>(c->st[c->cur], c->d_clk, c->n_init, c->steps > 0 ? 1 : 0,
-                                                          c->phys.mass,
+                                                          c->opt.precision ? 1 : 0, c->phys.mass,
                                                           c->phys.K, c->phys.G, c->phys.rho0, c0 * c0, c->twp.cp,
                                                           c->twp.T_init, c->d_energy + ENERGY_VALUES);
     k_energy_final<<<1, ENERGY_VALUES * 32, 0, c->stream>>>(c->d_energy + ENERGY_VALUES, nb, c->d_energy);

@@ -762,8 +762,10 @@ __device__ __noinline__ void prepare_tile(const BatchTable &T, TileSmem<LPP, W> 
                 const int c = e / CSROW, k = e - c * CSROW;
                 const int cx = G.X0 - 2 + c / HY, cy = G.Y0 - 2 + c % HY;
                 csv[r] = 0;
-                if (e < NHC * CSROW && k < G.nzr && cx >= 0 && cx < nx && cy >= 0 && cy < ny)
-                    csv[r] = first[(cx * ny + cy) * nz + G.zl + k];
+                if (e < NHC * CSROW && k < G.nzr && cx >= 0 && cx < nx && cy >= 0 && cy < ny) {
+                    const long long fi = (long long)(cx * ny + cy) * nz + G.zl + k;
+                    if (bounds_ok(a.clk, fi, (long long)P.num_cell + 1)) csv[r] = first[fi];
+                }
             }
 #pragma unroll
             for (int r = 0; r < NCS; r++) {
@@ -799,6 +801,9 @@ __device__ __noinline__ void prepare_tile(const BatchTable &T, TileSmem<LPP, W> 
                     const bool in = cx >= 0 && cx < nx && cy >= 0 && cy < ny;
                     len2[h] = in ? sm.cellstart[c][G.nzr - 1] - sm.cellstart[c][0] : 0;
                     sm.hstart[c] = sm.cellstart[c][0];
+                    // bounds-checked build: a column whose range lies outside
+                    // the record arrays is counted and not staged (len 0)
+                    if (!range_ok(a.clk, sm.hstart[c], len2[h], P.n_init)) len2[h] = 0;
                     sm.hlen[c] = len2[h];
                 }
                 const int i0 = group_scan<32>(len2[0], pl);

@@ -10,6 +10,8 @@
 // mfree_import_state rebuilds a context from it; the tools' triangle grids are
 // rebuilt from the meshes by the same code, so stepping the imported context
 // gives bitwise the results the exported one gives.
+#include <climits>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -187,6 +189,22 @@ int mfree_import_state(const void *buf, size_t size, void *stream, mfree_ctx **o
         return fail(MFREE_ERR_ARG, "mfree_import_state: exported by an incompatible version");
     if (h.total_bytes != size || h.n_init == 0) return fail(MFREE_ERR_ARG, "mfree_import_state: truncated or bad record");
     if (!r.get(&g, sizeof(g))) return fail(MFREE_ERR_ARG, "mfree_import_state: truncated record");
+    if (h.n_init >= uint64_t(INT_MAX)) return fail(MFREE_ERR_ARG, "mfree_import_state: bad particle count");
+    // the grid sizes the cell scratch and indexes the hash and the scans: a
+    // record whose sizes disagree would make the device read and write out of
+    // bounds, so it is refused
+    if (g.grid_set || g.grid_adaptive) {
+        // num_cell == nx * ny * nz, tested by division so that no product overflows
+        const bool dims_ok = g.nx > 0 && g.ny > 0 && g.nz > 0 && g.num_cell > 0 &&
+                             g.num_cell < int64_t(INT_MAX) / 2 && g.num_cell % g.nx == 0 &&
+                             (g.num_cell / g.nx) % g.ny == 0 && g.num_cell / g.nx / g.ny == g.nz;
+        const bool adaptive_ok = !g.grid_adaptive || (g.max_cell >= 2 && g.max_cell < int64_t(INT_MAX) / 2 &&
+                                                      g.num_cell < g.max_cell);
+        // an unlocked grid that has not stepped yet holds a placeholder cell edge of 0
+        const bool dx_ok = std::isfinite(g.g_dx) && (g.grid_adaptive ? g.g_dx >= 0.f : g.g_dx > 0.f);
+        if (!dims_ok || !adaptive_ok || !dx_ok)
+            return fail(MFREE_ERR_ARG, "mfree_import_state: inconsistent grid sizes in the record");
+    }
     std::unique_ptr<mfree_ctx> c;
     int st = alloc_ctx(int(h.n_init), (cudaStream_t)stream, c);
     if (st) return st;

@@ -15,6 +15,7 @@
 // the one array and it keeps the last call's contents: the per-cell counters
 // are cleared at the start of each call, and calls that overlap on the GPU
 // (different streams, or different host threads on one device) race on it.
+#include <atomic>
 #include <cstring>
 #include <string>
 
@@ -42,11 +43,20 @@ struct StaticScratch {
 // host it is only a stand-in), it passes the device address found below
 static __device__ __align__(256) StaticScratch g_static_scratch;
 
+// device address of the array, looked up once per device by the first call
+// on it (several host threads may make that first call at once: each finds
+// the same address, and the atomic makes the store and the later loads
+// well-defined).  After cudaDeviceReset the array lives at a new address the
+// cache does not know: a process that resets a device must not call this
+// entry point on that device again.
 constexpr int MAX_DEVICES = 64;
-StaticScratch *g_scratch_addr[MAX_DEVICES] = {nullptr};
+std::atomic<StaticScratch *> g_scratch_addr[MAX_DEVICES];
 
-// cell hash of plain positions: the step's kb_hash without blanking; a
-// particle outside the grid goes to the tail like a blanked one
+// cell hash of plain positions: the step's kb_hash without blanking.  A
+// position outside the grid, or with a NaN or infinite coordinate, goes to the
+// tail like a blanked particle.  As in the step (and the reference's
+// truncating (int) cast), a coordinate less than one cell below the grid's
+// lower corner still falls in cell 0 of that axis.
 __global__ void __launch_bounds__(HASH_BLOCK) k_hash_positions(StepArgs a, const float4 *pos, float bx, float by,
                                                                float bz) {
     const Params &P = a.p;
@@ -55,10 +65,11 @@ __global__ void __launch_bounds__(HASH_BLOCK) k_hash_positions(StepArgs a, const
     if (i < P.n_init) {
         const float4 p = pos[i];
         unsigned key = unsigned(P.num_cell);
+        const bool finite = isfinite(p.x) && isfinite(p.y) && isfinite(p.z);
         const int ix = int(__fdiv_rn(__fsub_rn(p.x, bx), P.gdx));
         const int iy = int(__fdiv_rn(__fsub_rn(p.y, by), P.gdx));
         const int iz = int(__fdiv_rn(__fsub_rn(p.z, bz), P.gdx));
-        if (ix >= 0 && ix < P.gnx && iy >= 0 && iy < P.gny && iz >= 0 && iz < P.gnz)
+        if (finite && ix >= 0 && ix < P.gnx && iy >= 0 && iy < P.gny && iz >= 0 && iz < P.gnz)
             key = unsigned((ix * P.gny + iy) * P.gnz + iz);
         a.s.key[i] = key;
         if (key < unsigned(P.num_cell)) atomicAdd(&a.s.count[key], 1);
@@ -94,14 +105,15 @@ extern "C" int mfree_cell_list_static(const float *pos4, int n, const float bbmi
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return sfail(MFREE_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= MAX_DEVICES) return sfail(MFREE_ERR_ARG, "mfree_cell_list_static: device index too large");
-    if (!g_scratch_addr[dev]) {  // set-up, once per device, with that device current
+    StaticScratch *S = g_scratch_addr[dev].load(std::memory_order_acquire);
+    if (!S) {  // set-up, once per device, with that device current
         void *ptr = nullptr;
         e = cudaGetSymbolAddress(&ptr, g_static_scratch);
         if (e != cudaSuccess || !ptr)
             return sfail(MFREE_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_scratch_addr[dev] = (StaticScratch *)ptr;
+        S = (StaticScratch *)ptr;
+        g_scratch_addr[dev].store(S, std::memory_order_release);
     }
-    StaticScratch *S = g_scratch_addr[dev];
     cudaStream_t s = (cudaStream_t)stream;
     StepArgs a{};
     a.p.n_init = n;

@@ -27,46 +27,29 @@ namespace mfree {
 namespace {
 
 using V = Vec3f;
-inline V add(V a, V b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-inline V sub(V a, V b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-inline V mul(float s, V a) { return {s * a.x, s * a.y, s * a.z}; }
-inline V neg(V a) { return {-a.x, -a.y, -a.z}; }
-inline bool eq(V a, V b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
-inline float dot(V a, V b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-inline V cross(V a, V b) { return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y}; }
-inline float length(V a) { return std::sqrt(dot(a, a)); }
+inline V add(V a, V b) { return vadd(a, b); }
+inline V sub(V a, V b) { return vsub(a, b); }
+inline V mul(float s, V a) { return vscale(s, a); }
+inline V neg(V a) { return vneg(a); }
+inline float dot(V a, V b) { return vdot(a, b); }
+inline V cross(V a, V b) { return vcross(a, b); }
+inline float length(V a) { return vlength(a); }
 inline V normalize(V a) { return mul(1.0f / std::sqrt(dot(a, a)), a); }
 inline float comp(V a, int d) { return d == 0 ? a.x : (d == 1 ? a.y : a.z); }
 inline void setc(V &a, int d, float v) { (d == 0 ? a.x : (d == 1 ? a.y : a.z)) = v; }
 
-V closest_on_segment(V p1, V p2, V p) {
-    float dx = p1.x - p2.x, dy = p1.y - p2.y, dz = p1.z - p2.z;
-    float ns2 = dx * dx + dy * dy + dz * dz;
-    if (ns2 == 0.f) return p1;
-    float t = ((p2.x - p1.x) * (p.x - p1.x) + (p2.y - p1.y) * (p.y - p1.y) + (p2.z - p1.z) * (p.z - p1.z)) / ns2;
-    if (t > 1.f) return p2;
-    if (t < 0.f) return p1;
-    return add(mul(1.f - t, p1), mul(t, p2));
-}
-
+// closest point on a triangle and the normal of the feature it lies on
+// (mesh_triangle::closest_point, surface_tri_mesh.cpp:42-104; the geometry is
+// shared with the contact kernel in mfree_geom.h)
 void closest_point(const HostTri &T, V qp, V &cp, V &np) {
-    V p1p2 = sub(T.p2, T.p1), p1p3 = sub(T.p3, T.p1), pp1 = sub(T.p1, qp);
-    float B = dot(p1p3, p1p2), E = dot(p1p2, p1p2), C = dot(p1p3, p1p3);
-    float det = B * B - E * C;
-    float A = dot(p1p3, pp1), D = dot(p1p2, pp1);
-    float t1 = (D * C - A * B) / det, t2 = (A * E - D * B) / det;
-    if (t1 < 0.f) {
-        cp = closest_on_segment(T.p1, T.p3, qp);
-        np = eq(cp, T.p1) ? T.np1 : (eq(cp, T.p3) ? T.np3 : T.ne3);
-    } else if (t2 < 0.f) {
-        cp = closest_on_segment(T.p1, T.p2, qp);
-        np = eq(cp, T.p1) ? T.np1 : (eq(cp, T.p2) ? T.np2 : T.ne1);
-    } else if (t1 + t2 > 1.f) {
-        cp = closest_on_segment(T.p2, T.p3, qp);
-        np = eq(cp, T.p2) ? T.np2 : (eq(cp, T.p3) ? T.np3 : T.ne2);
-    } else {
-        cp = add(add(T.p1, mul(t1, p1p2)), mul(t2, p1p3));
-        np = T.n;
+    switch (closest_on_triangle(T.p1, T.p2, T.p3, qp, cp)) {
+        case TF_V1: np = T.np1; break;
+        case TF_V2: np = T.np2; break;
+        case TF_V3: np = T.np3; break;
+        case TF_E12: np = T.ne1; break;
+        case TF_E23: np = T.ne2; break;
+        case TF_E31: np = T.ne3; break;
+        default: np = T.n; break;
     }
 }
 

@@ -4,11 +4,9 @@
 #include <string>
 #include <vector>
 
-namespace mfree {
+#include "mfree_geom.h"
 
-struct Vec3f {
-    float x, y, z;
-};
+namespace mfree {
 
 // mesh_triangle (surface_tri_mesh.h:39-63)
 struct HostTri {

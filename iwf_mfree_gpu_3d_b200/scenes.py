@@ -229,6 +229,33 @@ def orthogonal_cutting(nx: int = 40, ny: int = 20, nz: int = 10, dx: float = 1.0
         dt=dt, tools=[tool])
 
 
+def two_tool_scene(nx: int = 40, ny: int = 20, nz: int = 10, dx: float = 1.0e-3, v_tool: float = 1.0e-3,
+                   depths=(5.0, 3.0), engage=(0.05, 0.3), **kw) -> Scene:
+    """Two rigid wedges cutting one block side by side, the way the
+    reference's multi-grain setups step several tools in one contact pass
+    (benchmarks_single_grain.cu:29-471; tools processed in order,
+    leap_frog.cu:178-181): the first wedge covers the -y half of the block at
+    depths[0]*dx, the second the +y half at depths[1]*dx, a dx apart.  Both
+    move towards -x at v_tool; the grid and blanking box cover both."""
+    sc = orthogonal_cutting(nx, ny, nz, dx, v_tool=v_tool, depth=depths[0], engage=engage[0], **kw)
+    lx = (nx - 1) * dx
+    ly = ny * dx
+    halves = ((-ly / 2.0 - 2.0 * dx, -0.5 * dx), (0.5 * dx, ly / 2.0 + 2.0 * dx))
+    algorithm = sc.tools[0].algorithm
+    sc.tools = []
+    for (y0, y1), depth, eng in zip(halves, depths, engage):
+        verts, tris = wedge_tool(x_edge=lx - eng * dx, z_edge=-depth * dx, y0=y0, y1=y1, dx=dx)
+        sc.tools.append(Tool(verts=verts, tris=tris, vel=np.array([-v_tool, 0.0, 0.0], np.float32),
+                             mu=0.35, contact_alpha=0.1, algorithm=algorithm))
+    pad = 15.0 * dx
+    allv = np.concatenate([t.verts for t in sc.tools])
+    lo = (np.minimum(sc.pos[:, :3].min(0), allv.min(0)) - pad).astype(np.float32)
+    hi = (np.maximum(sc.pos[:, :3].max(0), allv.max(0)) + pad).astype(np.float32)
+    sc.grid_bbmin, sc.grid_bbmax, sc.blank_bbmin, sc.blank_bbmax = lo, hi, lo.copy(), hi.copy()
+    sc.name = f"two_tools_{nx}x{ny}x{nz}"
+    return sc
+
+
 def small_scene(**kw) -> Scene:
     """40 x 20 x 10 = 8,000 particles, Brookshaw, no CSPM (the 8k workload)."""
     return orthogonal_cutting(40, 20, 10, **kw)

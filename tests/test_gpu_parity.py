@@ -11,7 +11,7 @@ import pytest
 import oracle
 from iwf_mfree_gpu_3d_b200 import api, scenes
 
-from helpers import compare, gpu_state, oracle_state
+from helpers import check, compare, gpu_state, oracle_state
 
 pytestmark = pytest.mark.gpu
 
@@ -87,10 +87,7 @@ def test_three_steps_against_fp64_oracle_full_size_1m():
         orc.step()
     err = compare(gpu_state(sim), oracle_state(orc), sc)
     print("1M, 3-step relative L2 (FP32 CUDA vs FP64 oracle):", err)
-    assert err["blank_mismatch"] == 0
-    tol = dict(POS=5e-3, VEL=5e-3, S=5e-3, EPS_PL=2e-2, T=2e-2, RHO=5e-3)
-    for k, v in tol.items():
-        assert err[k] < v, (k, err)
+    check(err, "1m_3")
     sim.close()
 
 
@@ -99,8 +96,8 @@ def test_100_steps_against_fp64_oracle_full_size_1m_plain_and_precision():
     after 100 steps, run once in plain FP32 and once in the precision form
     (compensated hi/lo positions and velocities), each against one FP64
     oracle run: the per-field relative L2 error of both is printed, both stay
-    within the tolerances of the 8,000-particle 100-step test, and the
-    precision form's displacement error is no worse than plain FP32's."""
+    within its tolerances, and the precision form's displacement error is at
+    most a tenth of plain FP32's (measured: 0.019)."""
     sc = scenes.million_scene()
     plain = _sim(sc)
     prec = _sim(sc, precision=1)
@@ -115,12 +112,9 @@ def test_100_steps_against_fp64_oracle_full_size_1m_plain_and_precision():
     for name, err in (("plain FP32", e_plain), ("precision form", e_prec)):
         print(f"1M, 100-step relative L2 vs FP64 oracle, {name}: " +
               ", ".join(f"{k} {v:.3e}" for k, v in err.items()))
-    tol = dict(POS=5e-3, VEL=5e-3, S=5e-3, EPS_PL=2e-2, T=2e-2, RHO=5e-3)
-    for err in (e_plain, e_prec):
-        assert err["blank_mismatch"] == 0
-        for k, v in tol.items():
-            assert err[k] < v, (k, err)
-    assert e_prec["POS"] <= 1.5 * e_plain["POS"]
+    check(e_plain, "1m_100")
+    check(e_prec, "1m_100_prec")
+    assert e_prec["POS"] <= 0.1 * e_plain["POS"]
     plain.close()
     prec.close()
 
@@ -152,10 +146,7 @@ def test_100_steps_against_fp64_oracle_8k():
         orc.step()
     err = compare(gpu_state(sim), oracle_state(orc), sc)
     print("100-step relative L2 (FP32 CUDA vs FP64 oracle):", err)
-    assert err["blank_mismatch"] == 0
-    tol = dict(POS=5e-3, VEL=5e-3, S=5e-3, EPS_PL=2e-2, T=2e-2, RHO=5e-3)
-    for k, v in tol.items():
-        assert err[k] < v, (k, err)
+    check(err, "8k_100")
     sim.close()
 
 

@@ -8,7 +8,7 @@ import pytest
 import oracle
 from iwf_mfree_gpu_3d_b200 import api, scenes
 
-from helpers import compare, gpu_state, oracle_state
+from helpers import check, compare, gpu_state, oracle_state
 
 pytestmark = pytest.mark.gpu
 
@@ -29,15 +29,15 @@ def test_cspm_pse_100_steps():
     sim, orc = _run(sc, 100)
     err = compare(gpu_state(sim), oracle_state(orc), sc)
     print("CSPM+PSE 100-step relative L2:", err)
-    assert err["blank_mismatch"] == 0
-    for k, v in dict(POS=5e-3, VEL=5e-3, S=5e-3, EPS_PL=2e-2, T=2e-2, RHO=5e-3).items():
-        assert err[k] < v, (k, err)
+    check(err, "cspm_pse_100")
     sim.close()
 
 
 def test_precision_form_tracks_fp64_closer():
     """Compensated hi/lo positions and velocities: the displacement error
-    against the FP64 oracle is no worse than plain FP32's."""
+    against the FP64 oracle is at most a fifth of plain FP32's (measured:
+    0.12) after 60 steps, and position and velocity stay within three times
+    their measured errors (1.0e-5, 1.4e-5)."""
     sc = scenes.small_scene()
     plain, orc = _run(sc, 60)
     prec = api.Simulation.from_scene(sc, precision=1)
@@ -47,8 +47,8 @@ def test_precision_form_tracks_fp64_closer():
     e_plain = compare(gpu_state(plain), o, sc)
     e_prec = compare(gpu_state(prec, f64=True), o, sc)
     print("plain:", e_plain["POS"], e_plain["VEL"], "precision form:", e_prec["POS"], e_prec["VEL"])
-    assert e_prec["POS"] < 5e-3 and e_prec["VEL"] < 5e-3
-    assert e_prec["POS"] <= 1.5 * e_plain["POS"]
+    assert e_prec["POS"] < 3.2e-5 and e_prec["VEL"] < 4.2e-5
+    assert e_prec["POS"] <= 0.2 * e_plain["POS"]
     plain.close()
     prec.close()
 
@@ -58,8 +58,58 @@ def test_exhaustive_contact_algorithm():
     sim, orc = _run(sc, 30)
     err = compare(gpu_state(sim), oracle_state(orc), sc)
     print("exhaustive contact 30-step relative L2:", err)
-    for k, v in dict(POS=5e-3, VEL=5e-3, S=5e-3, FC=2e-2).items():
-        assert err[k] < v, (k, err)
+    check(err, "exhaustive_30")
+    sim.close()
+
+
+def _force_series(sc, steps):
+    """Tool forces recorded on every step (tool_forces::get_forces_host,
+    tool_3d_gpu.cu:30-69) by the CUDA path and the FP64 oracle."""
+    sim = api.Simulation.from_scene(sc)
+    orc = oracle.Oracle(sc, prec=64)
+    fg, fo = [], []
+    for _ in range(steps):
+        sim.step(record_forces=True)
+        orc.step(record=True)
+        fg.append(sim.tool_forces().astype(np.float64).copy())
+        fo.append(orc.tool_forces().astype(np.float64).copy())
+    return sim, orc, np.array(fg), np.array(fo)
+
+
+def test_tool_forces_match_oracle_over_100_steps():
+    """The summed tool force of every step against the FP64 oracle's over 100
+    steps: the force series (relative L2 over steps and components), the
+    impulse (the sum over steps) and the steps on which the tool touches."""
+    sc = scenes.small_scene()
+    sim, orc, fg, fo = _force_series(sc, 100)
+    touch_g, touch_o = np.abs(fg).sum(axis=2) > 0, np.abs(fo).sum(axis=2) > 0
+    e_series = np.linalg.norm(fg - fo) / np.linalg.norm(fo)
+    e_impulse = np.linalg.norm(fg.sum(0) - fo.sum(0)) / np.linalg.norm(fo.sum(0))
+    print(f"tool forces over 100 steps: series rel L2 {e_series:.3e}, impulse {e_impulse:.3e}, "
+          f"contact steps {touch_g.sum()} (oracle {touch_o.sum()})")
+    assert touch_o.sum() > 20
+    # contact starts and ends where a particle crosses the tool surface: a
+    # last-bit difference may move one such step
+    assert int((touch_g != touch_o).sum()) <= 2
+    # measured: series 2.8e-5, impulse 8.6e-6
+    assert e_series < 1e-4 and e_impulse < 3e-5
+    sim.close()
+
+
+def test_two_tools_against_fp64_oracle():
+    """Two wedges at different depths cutting one block side by side (the
+    reference's multi-tool stepping, tools processed in order): every field
+    after 100 steps and each tool's force series against the FP64 oracle."""
+    sc = scenes.two_tool_scene()
+    sim, orc, fg, fo = _force_series(sc, 100)
+    err = compare(gpu_state(sim), oracle_state(orc), sc)
+    print("two tools 100-step relative L2:", err)
+    check(err, "two_tools_100")
+    for k in range(2):
+        assert (np.abs(fo[:, k]).sum(axis=1) > 0).sum() > 5, k  # both tools touch the block
+        e_series = np.linalg.norm(fg[:, k] - fo[:, k]) / np.linalg.norm(fo[:, k])
+        print(f"tool {k}: force series rel L2 {e_series:.3e}")
+        assert e_series < 1e-4, (k, e_series)  # measured 2.7e-5 and 4.5e-6
     sim.close()
 
 
@@ -78,8 +128,7 @@ def test_tool_particles_conduct_heat():
     g, o = gpu_state(sim), oracle_state(orc)
     err = compare(g, o, sc)
     print("tool particles 40-step relative L2:", err)
-    for k, v in dict(POS=5e-3, VEL=5e-3, T=2e-2).items():
-        assert err[k] < v, (k, err)
+    check(err, "tool_particles_40")
     # tool particles moved rigidly with the tool velocity
     ids = sim.get("ID")
     pos = np.empty((n, 4), np.float32)
@@ -102,9 +151,7 @@ def test_single_grain_with_tool_particles_against_oracle():
     g, o = gpu_state(sim), oracle_state(orc)
     err = compare(g, o, sc)
     print("single grain 40-step relative L2:", err)
-    assert err["blank_mismatch"] == 0
-    for k, v in dict(POS=5e-3, VEL=5e-3, S=5e-3, EPS_PL=2e-2, T=2e-2, RHO=5e-3).items():
-        assert err[k] < v, (k, err)
+    check(err, "grain_40")
     sim.close()
 
 
@@ -261,17 +308,22 @@ def test_compact_arrays_match_the_reference_layout_fields():
         s.close()
 
 
-def test_fp64_energy_and_cfl_reductions_match_the_fields():
+@pytest.mark.parametrize("precision", [0, 1])
+def test_fp64_energy_and_cfl_reductions_match_the_fields(precision):
     """mfree_get_energies: FP64 device reductions of the current state against
     the same sums in numpy FP64 from the fields; repeated calls give the same
-    bits."""
-    sc = scenes.small_scene()
+    bits.  In the precision form the velocity is hi + lo of the compensated
+    accumulation (the FP64 field read)."""
+    sc = scenes.small_scene(precision=precision)
     sim = api.Simulation.from_scene(sc)
     sim.advance(20, use_graph=True)
     e1, e2 = sim.energies(), sim.energies()
     assert e1 == e2
     n_act = sim.counts()[0]
-    vel = sim.get("VEL")[:n_act, :3].astype(np.float64)
+    vel = sim.get64("VEL")[:n_act, :3] if precision else sim.get("VEL")[:n_act, :3].astype(np.float64)
+    if precision:  # the low parts are in the sum: hi alone differs
+        hi = sim.get("VEL")[:n_act, :3].astype(np.float64)
+        assert np.any(vel != hi)
     rho = sim.get("RHO")[:n_act].astype(np.float64)
     S = sim.get("S").reshape(-1, 9)[:n_act].astype(np.float64)
     T = sim.get("T")[:n_act].astype(np.float64)

@@ -17,7 +17,7 @@ import pytest
 import oracle
 from iwf_mfree_gpu_3d_b200 import api, scenes, serve
 
-from helpers import compare, oracle_state
+from helpers import TOL, compare, oracle_state
 
 pytestmark = pytest.mark.gpu
 
@@ -70,8 +70,7 @@ def test_sampled_request_matches_fp64_oracle_at_step_100():
     g["BLANKED"] = o["BLANKED"]
     err = compare(g, o, sc, names=["POS", "VEL", "S", "EPS_PL", "T", "RHO"])
     print("served request vs FP64 oracle, relative L2 at step 100:", err)
-    tol = dict(POS=5e-3, VEL=5e-3, S=5e-3, EPS_PL=2e-2, T=2e-2, RHO=5e-3)
-    for k, v in tol.items():
+    for k, v in TOL["served_100"].items():
         assert err[k] < v, (k, err)
 
 
