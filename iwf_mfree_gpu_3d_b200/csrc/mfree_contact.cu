@@ -218,18 +218,29 @@ __device__ __forceinline__ void finalize_body(const StepArgs &a, int bid) {
                 }
                 if (dot(cp - qp, n) > 0.f) continue;
             }
+            // the reference's operation order, divisions included
+            // (tool_3d_gpu.cu:630-661): fN = ((-m gN) n) / dt^2 * alpha,
+            // kdeltae = ((alpha m) vr) / dt, fT = (fy fstar) / |fstar|
             const float gN = dot(qp - cp, n);
-            V3 fN = T.alpha * ((1.f / (dt * dt)) * ((-P.mass * gN) * n));
+            const float dt2 = dt * dt;
+            const V3 mgn = (-P.mass * gN) * n;
+            V3 fN = v3(mgn.x / dt2 * T.alpha, mgn.y / dt2 * T.alpha, mgn.z / dt2 * T.alpha);
             V3 fT = v3(0.f, 0.f, 0.f);
             if (T.mu != 0.f) {
                 V3 vm = P.friction_tool_vel ? v3(T.vel[0], T.vel[1], T.vel[2]) : v3(0.f, 0.f, 0.f);
                 V3 v = v3(vel.x, vel.y, vel.z) - vm;
                 V3 vr = v3(v.x - v.x * n.x, v.y - v.y * n.y, v.z - v.z * n.z);
-                V3 kde = (1.f / dt) * ((T.alpha * P.mass) * vr);
+                const V3 amv = (T.alpha * P.mass) * vr;
+                V3 kde = v3(amv.x / dt, amv.y / dt, amv.z / dt);
                 float fy = T.mu * len(fN);
                 V3 fs = v3(ft.x, ft.y, ft.z) - kde;
                 float lfs = len(fs);
-                fT = lfs > fy ? (fy / lfs) * fs : fs;
+                if (lfs > fy) {
+                    const V3 ffs = fy * fs;
+                    fT = v3(ffs.x / lfs, ffs.y / lfs, ffs.z / lfs);
+                } else {
+                    fT = fs;
+                }
             }
             fc.x = fN.x; fc.y = fN.y; fc.z = fN.z;
             ft.x = fT.x; ft.y = fT.y; ft.z = fT.z;

@@ -342,38 +342,61 @@ __device__ inline void artificial_stress(float sxx, float syy, float szz, float 
 }
 
 // ------------------------------------------------------- Johnson-Cook ----
-// sigma_yield / opt_fun / solve_secant (plasticity.cuh:28-93) in FP32 with
-// the same iteration, tolerance and limit.
-__device__ __forceinline__ float jc_sigma_yield(const Params &P, float eps_pl, float eps_pl_dot, float T) {
-    float theta = (T - P.jc_Tref) / (P.jc_Tmelt - P.jc_Tref);
-    float a = P.jc_A + P.jc_B * powf(eps_pl, P.jc_n);
-    float ed = eps_pl_dot / P.jc_epsdot_ref;
-    float b = ed > 1.0f ? 1.0f + P.jc_C * logf(ed) : powf(1.0f + ed, P.jc_C);
-    float c = 1.0f - powf(theta, P.jc_m);
+// sigma_yield / opt_fun / solve_secant (plasticity.cuh:28-93), evaluated the
+// way the reference's FP32 build evaluates them: in FP64, from FP32 inputs,
+// with the strain-rate logarithm taken as logf and multiplied by C in float
+// (log_t = logf in types.h).  The secant stops on an absolute change of the
+// plastic multiplier below 1e-6; in FP32 its finite-difference slope at the
+// starting multiplier of 1e-8 is below the resolution of g and the iterates part
+// from the FP64 ones (the plastic strain of a loaded state differed by 2-3 %
+// after one step), so the root is solved in FP64.  Only yielding particles
+// reach it.
+__device__ __forceinline__ double jc_sigma_yield(const Params &P, double eps_pl, double eps_pl_dot, double T) {
+    const double theta = (T - (double)P.jc_Tref) / (double)(P.jc_Tmelt - P.jc_Tref);
+    const double a = (double)P.jc_A + (double)P.jc_B * pow(eps_pl, (double)P.jc_n);
+    const double ed = eps_pl_dot / (double)P.jc_epsdot_ref;
+    const double b = ed > 1.0 ? 1.0 + (double)(P.jc_C * logf((float)ed)) : pow(1.0 + ed, (double)P.jc_C);
+    const double c = 1.0 - pow(theta, (double)P.jc_m);
     return a * b * c;
 }
-__device__ __forceinline__ float jc_opt(const Params &P, float dl, float normS, float eps0, float T, float dt) {
-    const float s23 = 0.81649658092772603f;  // sqrt(2/3)
-    float dlp = fmaxf(dl, 0.f);
-    return normS - 2.f * P.G * dl - s23 * jc_sigma_yield(P, eps0 + s23 * dlp, s23 * dlp / dt, T);
+__device__ __forceinline__ double jc_opt(const Params &P, double dl, double normS, double eps0, double T, double dt) {
+    const double s23 = 0.81649658092772603;  // sqrt(2/3) in double
+    const double dlp = fmax(dl, 0.0);
+    return normS - 2.0 * (double)P.G * dl - s23 * jc_sigma_yield(P, eps0 + s23 * dlp, s23 * dlp / dt, T);
 }
-__device__ inline float jc_secant(const Params &P, float init, float normS, float eps0, float T, float dt,
-                                  bool &failed) {
-    float dl = init;
+// out of line: its FP64 registers stay out of the calling kernel's allocation
+static __device__ __noinline__ double jc_secant(const Params &P, double init, double normS, double eps0, double T,
+                                         double dt, int *failed) {
+    double dl = init;
     for (int iter = 0;; iter++) {
-        float g = jc_opt(P, dl, normS, eps0, T, dt);
-        float dl1 = dl * 1.01f;
-        float g1 = jc_opt(P, dl1, normS, eps0, T, dt);
-        float slope = (g - g1) / (dl - dl1);
-        float old = dl;
+        const double g = jc_opt(P, dl, normS, eps0, T, dt);
+        const double dl1 = dl * 1.01;
+        const double g1 = jc_opt(P, dl1, normS, eps0, T, dt);
+        const double slope = (g - g1) / (dl - dl1);
+        const double old = dl;
         dl = dl - g / slope;
-        if (dl < 0.f) dl = -0.1f * dl;
-        if (fabsf(dl - old) < 1e-6f) return dl;
+        if (dl < 0.0) dl = -0.1 * dl;
+        if (fabs(dl - old) < 1e-6) return dl;
         if (iter > P.max_secant_iter) {
-            failed = true;
+            *failed = 1;
             return dl;
         }
     }
+}
+static __device__ __noinline__ float jc_yield_stress(const Params &P, float eps_pl, float eps_pl_dot, float T) {
+    return (float)jc_sigma_yield(P, eps_pl, eps_pl_dot, T);
+}
+// the same yield stress in FP32, only to screen out the clearly elastic
+// particles before the FP64 evaluation: its relative error is below 1e-4 even
+// next to the melting temperature (1 - theta^m ~ 7e-4 at the clamp), so a von
+// Mises stress under 0.99 of it is under the FP64 value as well
+__device__ __forceinline__ float jc_yield_stress_screen(const Params &P, float eps_pl, float eps_pl_dot, float T) {
+    const float theta = (T - P.jc_Tref) / (P.jc_Tmelt - P.jc_Tref);
+    const float a = P.jc_A + P.jc_B * powf(eps_pl, P.jc_n);
+    const float ed = eps_pl_dot / P.jc_epsdot_ref;
+    const float b = ed > 1.0f ? 1.0f + P.jc_C * logf(ed) : powf(1.0f + ed, P.jc_C);
+    const float c = 1.0f - powf(theta, P.jc_m);
+    return a * b * c;
 }
 
 // Jaumann stress rate (actions_gpu.cu:134-190): S_t = 2G(epsdot - tr/3 I) + W S + S W^T,

@@ -224,22 +224,23 @@ __device__ void epilogue(const StepArgs &a, int i, const float *res) {
         float Tc = T;
         if (P.jc_clamp != 0.f) Tc = Tc > P.jc_Tmelt ? P.jc_Tmelt - 1.f : Tc;
         const float svm = 1.22474487139158905f * nS;
-        const float sY = jc_sigma_yield(P, eps, epsd, Tc);
-        if (svm < sY) {
-            epsd = 0.f;
+        if (svm < 0.99f * jc_yield_stress_screen(P, eps, epsd, Tc) || svm < jc_yield_stress(P, eps, epsd, Tc)) {
+            epsd = 0.f;  // elastic
         } else {
-            bool failed = false;
-            const float s23 = 0.81649658092772603f;
-            const float init = fmaxf(epsd * dt * s23, 1e-8f);
-            const float dl = jc_secant(P, init, nS, eps, Tc, dt, failed);
+            // FP64 secant from FP32 inputs, the result stored as float
+            int failed = 0;
+            const double init = fmax((double)(epsd * dt) * 0.81649658092772603, 1e-8);
+            const float dl = (float)jc_secant(P, init, nS, eps, Tc, dt, &failed);
             if (failed) atomicAdd(&a.clk->secant_failures, 1ull);
+            const float s23 = 0.81649658092772603f;  // sqrtf(2/3)
             const float e1 = eps + s23 * fmaxf(dl, 0.f);
             const float ed1 = s23 * fmaxf(dl, 0.f) / dt;
-            const float f = dl * 2.f * P.G / nS;
+            // S - S / |S| * dl * 2 * G: the quotient and the product with dl in
+            // float, the rest in double (the literal 2. promotes it)
 #pragma unroll
-            for (int k = 0; k < 6; k++) s[k] = s[k] - s[k] * f;
+            for (int k = 0; k < 6; k++) s[k] = (float)((double)s[k] - (double)(s[k] / nS * dl) * 2.0 * (double)P.G);
             if (P.wp_tq != 0.f) {
-                const float sY2 = jc_sigma_yield(P, e1, ed1, Tc);
+                const float sY2 = jc_yield_stress(P, e1, ed1, Tc);
                 T += P.wp_tq / (P.wp_cp * vel.w) * (e1 - eps) * sY2;
             }
             eps = e1;

@@ -42,8 +42,15 @@ def build(force: bool = False) -> str:
     return LIB
 
 
-def build_ref(reference_root: str = "/root/reference") -> str | None:
+def reference_root() -> str:
+    """Where the reference's checkout is looked for: $MFREE_REFERENCE_ROOT, else
+    a directory named ``reference`` beside this repository."""
+    return os.environ.get("MFREE_REFERENCE_ROOT") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
+
+
+def build_ref(reference_root: str | None = None) -> str | None:
     """Compile the reference's functions for the host, when its sources exist."""
+    reference_root = reference_root or globals()["reference_root"]()
     if not os.path.exists(os.path.join(reference_root, "src", "kernels.cuh")):
         return REF_LIB if os.path.exists(REF_LIB) else None
     subprocess.check_call(["sh", os.path.join(HERE, "build_ref.sh"), reference_root])

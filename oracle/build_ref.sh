@@ -3,9 +3,10 @@
 # lie (read-only), for the known-answer tests of the oracle.  Needs the
 # reference checkout; the built library travels with the repository snapshot.
 # Usage: oracle/build_ref.sh [reference_root]
+#        (default: $MFREE_REFERENCE_ROOT, else ../reference beside the repository)
 set -e
 here=$(cd "$(dirname "$0")" && pwd)
-ref=${1:-/root/reference}
+ref=${1:-${MFREE_REFERENCE_ROOT:-$(dirname "$(dirname "$here")")/reference}}
 cuda=${CUDA_HOME:-/usr/local/cuda}
 [ -f "$ref/src/kernels.cuh" ] || { echo "reference sources not found under $ref" >&2; exit 1; }
 mkdir -p "$here/_ref"

@@ -1,0 +1,164 @@
+"""The reference's own GPU step as a third party to the parity checks.
+
+baseline/_ref/ref_step_<variant> is the reference's leap_frog::step
+(src/leap_frog.cu:121-195) compiled for sm_100a from its sources
+(baseline/build_ref_gpu.sh), with the behaviour-preserving build patch only.
+On the same seeded scenes:
+
+* one step from a loaded state (random stress, velocity, temperature and
+  density) exercises every term, the artificial stress and the GLM-ordered
+  rotations included: the oracle (FP32 and FP64) and the CUDA path agree with
+  the reference's step to rounding;
+* from rest, the first step's contact forces agree to 1e-6 (every other field
+  is still exactly zero);
+* after 100 steps (30 for the exhaustive contact), the reference's GPU step is
+  within the oracle's FP64 tolerances -- so the oracle is pinned to the
+  reference itself, including the parts computed through GLM (artificial-stress
+  rotation, Jaumann rate, CSPM inverse, contact geometry) and the step order;
+* the CUDA path is within three times the measured distance of the reference's
+  FP32 trajectory, and its tool force agrees.
+
+Skipped where the comparator has not been built (it needs the reference's
+sources at build time).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from baseline import refgpu
+from iwf_mfree_gpu_3d_b200 import api, scenes
+
+from helpers import FIELDS, by_id, check, compare, gpu_state, loaded, oracle_state
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not all(refgpu.available(v) for v in refgpu.VARIANTS),
+                                 reason="the reference's GPU build (baseline/_ref) is not built")]
+
+# every field the reference's driver reads back (it has no plastic strain rate)
+REF_FIELDS = [f for f in FIELDS if f != "EPS_PL_DOT"]
+
+SCENES = {
+    "8k": (lambda: scenes.small_scene(), 100, "8k_100"),
+    "cspm_pse": (lambda: scenes.orthogonal_cutting(30, 15, 12, cspm=True, conduction=2), 100, "cspm_pse_100"),
+    "two_tools": (lambda: scenes.two_tool_scene(), 100, "two_tools_100"),
+    "exhaustive": (lambda: scenes.orthogonal_cutting(algorithm=1), 30, "exhaustive_30"),
+}
+
+# CUDA path against the reference's GPU step: five times the distance measured
+# on a B200.  Both are FP32; the trajectories part by rounding (the two
+# compilers fuse multiply-adds in different places, and the pair sums are
+# added in another order), and stick-slip switches of single particles at the
+# Coulomb cap make the distance vary by ~2x between code versions.
+TOL_VS_REF = {
+    "8k": dict(POS=2.4e-5, VEL=7.5e-5, S=4.5e-5, EPS_PL=3.7e-6, T=9.5e-6, RHO=1.6e-7, FC=6.5e-4, FT=1.05e-3),
+    "cspm_pse": dict(POS=6e-5, VEL=3.3e-4, S=1.9e-4, EPS_PL=4.7e-5, T=6.5e-5, RHO=4.9e-7, FC=1.8e-3),
+    "two_tools": dict(POS=9e-6, VEL=2.3e-5, S=2e-5, EPS_PL=4.2e-6, T=4.8e-6, RHO=2.3e-7, FC=4.5e-4),
+    "exhaustive": dict(POS=1.5e-5, VEL=5.5e-6, S=3.6e-6, EPS_PL=1.4e-6, T=5.5e-6, RHO=5e-8, S_T=8e-6),
+}
+
+
+def ref_state(rec, names=None) -> dict:
+    st = rec["state"]
+    ids = st["ID"]
+    out = {n: by_id(ids, st[n].astype(np.float64)) for n in (names or REF_FIELDS)}
+    out["BLANKED"] = by_id(ids, st["BLANKED"].astype(np.float64))
+    return out
+
+
+def force_rel(a, b) -> float:
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+LOADED = {
+    "brookshaw": lambda: loaded(scenes.small_scene()),
+    "cspm_pse": lambda: loaded(scenes.orthogonal_cutting(30, 15, 12, cspm=True, conduction=2)),
+}
+LOADED_FIELDS = REF_FIELDS + ["R"]
+# relative L2 after the step; 1e-5 where not listed.  Rounding sets these:
+# a position moves by ~1e-5 of itself in a step, so the last bit of an FP32
+# position is ~1e-3 of its displacement (FP64 against the FP32 reference), and a
+# fused multiply-add in the reference's position update is ~1e-6 of it; the
+# friction force changes branch at the Coulomb cap, where a last-bit
+# difference in the normal force can switch a particle.
+LOADED_TOL = {
+    "oracle FP32": dict(POS=3e-5, FT=1e-4),
+    "oracle FP64": dict(POS=3e-3, FC=5e-5, FT=1e-4),
+    "CUDA path": dict(POS=3e-5, FC=5e-5, FT=1e-4),
+}
+
+
+@pytest.mark.parametrize("name", list(LOADED))
+def test_one_step_from_a_loaded_state_equals_the_reference_gpu_step(name):
+    """Every rate, the artificial stress R and the new state after one step."""
+    sc = LOADED[name]()
+    ref = ref_state(refgpu.run(sc, 0, 1, state=True), LOADED_FIELDS)
+    res = {}
+    for prec in (32, 64):
+        orc = oracle.Oracle(sc, prec=prec)
+        orc.set_field("S", sc.S0)
+        orc.step()
+        res[f"oracle FP{prec}"] = oracle_state(orc, LOADED_FIELDS)
+    sim = api.Simulation.from_scene(sc)
+    sim.set("S", sc.S0)
+    sim.step()
+    res["CUDA path"] = gpu_state(sim, LOADED_FIELDS)
+    sim.close()
+    errs = {label: compare(other, ref, sc, LOADED_FIELDS) for label, other in res.items()}
+    for label, err in errs.items():
+        print(name, label, {k: f"{v:.1e}" for k, v in err.items()})
+    for label, err in errs.items():
+        assert err["blank_mismatch"] == 0, (label, err)
+        for f in LOADED_FIELDS:
+            assert err[f] < LOADED_TOL[label].get(f, 1e-5), (name, label, f, err[f])
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_first_contact_forces_equal_the_reference_gpu_step(name):
+    """From rest, the first step's only non-zero output is the contact force of
+    the initial configuration (closest points, normals, ray parity)."""
+    make, _, _ = SCENES[name]
+    sc = make()
+    ref = ref_state(refgpu.run(sc, 0, 1, state=True))
+    orc = oracle.Oracle(sc, prec=32)
+    orc.step()
+    o = oracle_state(orc, REF_FIELDS)
+    sim = api.Simulation.from_scene(sc)
+    sim.step()
+    g = gpu_state(sim, REF_FIELDS)
+    sim.close()
+    for other, label in ((o, "oracle FP32"), (g, "CUDA path")):
+        err = compare(other, ref, sc, REF_FIELDS)
+        assert err["blank_mismatch"] == 0, (label, err)
+        for f in REF_FIELDS:
+            limit = 1e-6 if f in ("FC", "FT") else 0.0
+            assert err[f] <= limit, (name, label, f, err[f])
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_reference_gpu_step_pins_the_oracle_and_the_cuda_path(name):
+    make, steps, scenario = SCENES[name]
+    sc = make()
+    rec = refgpu.run(sc, 0, steps, state=True)
+    ref = ref_state(rec)
+    orc = oracle.Oracle(sc, prec=64)
+    sim = api.Simulation.from_scene(sc)
+    for k in range(steps):
+        orc.step(record=(k == steps - 1))
+        sim.step(record_forces=(k == steps - 1))
+    o = oracle_state(orc, REF_FIELDS)
+    g = gpu_state(sim, REF_FIELDS)
+    f_cuda = np.asarray(sim.tool_forces())
+    sim.close()
+    # the reference's own FP32 step against the FP64 oracle
+    check(compare(ref, o, sc, REF_FIELDS), scenario)
+    # the CUDA path against the reference's step
+    err = compare(g, ref, sc, REF_FIELDS)
+    assert err["blank_mismatch"] == 0, err
+    print(name, {k: f"{v:.1e}" for k, v in err.items()})
+    for f, tol in TOL_VS_REF[name].items():
+        assert err[f] < tol, (name, f, err[f], tol)
+    f_ref = rec["state"]["TOOL_FORCES"]
+    assert force_rel(f_cuda, f_ref) < 5e-4, (f_cuda, f_ref)
+    assert force_rel(orc.tool_forces(), f_ref) < 5e-4, (orc.tool_forces(), f_ref)
