@@ -29,8 +29,15 @@ At N = 1 the line also carries the two systems forms, measured live:
     150 GB budget, with p50/p99 latency (arrival to result) and throughput;
     rate, duration, sizes and step counts are scaled down so the run takes
     seconds (the scaling is stated in the line).
-  * "precision_form" (1M workload): the same step in the precision form.
+  * "precision_form" (1M workload): the same step in the precision form;
+  * "grain": the single-grain configuration (400 x 160 x 64 block plus the
+    grain's tool particles, ~4.1M, compensated positions): particle-steps/s and
+    HBM GB/s.
 --no-extras skips these.
+
+Beside the main line (and the grain leg), "reference_gpu" times the
+reference's own GPU step -- leap_frog::step built for sm_100a from its
+sources by baseline/build_ref_gpu.sh -- on the same scene and GPU.
 """
 from __future__ import annotations
 
@@ -77,11 +84,15 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving measurements")
     ap.add_argument("--batch-scenes", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=20)
-    ap.add_argument("--serve-rate", type=float, default=4.0, help="requests per second")
-    ap.add_argument("--serve-seconds", type=float, default=20.0, help="arrival window")
-    ap.add_argument("--serve-nmax", type=int, default=100000, help="largest request (particles)")
-    ap.add_argument("--serve-steps", type=int, nargs=2, default=[50, 500], help="steps per request, range")
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="requests per second")
+    ap.add_argument("--serve-seconds", type=float, default=30.0, help="arrival window")
+    ap.add_argument("--serve-nmax", type=int, default=500000, help="largest request (particles)")
+    ap.add_argument("--serve-step-scale", type=float, default=0.1,
+                    help="factor on every request's U[500, 5000] step count")
     ap.add_argument("--serve-chunk", type=int, default=25, help="steps between admissions")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the reference's own GPU step (baseline/_ref) on the same scene")
+    ap.add_argument("--no-grain", action="store_true", help="skip the single-grain leg")
     return ap.parse_args()
 
 
@@ -416,14 +427,65 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
             "counters": counters,
             "hbm": hbm_roofline(value, sc),
             "hbm_kernels": kernel_hbm(sc, n_act, step_ms_dev)}
+    if world == 1 and not args.no_reference_gpu:
+        line["reference_gpu"] = run_reference_gpu(sc, ms / args.steps, e2e)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.workload)
+    if world == 1 and not args.no_extras and not args.no_grain and args.workload != "grain":
+        line["grain"] = run_grain(args, opts)
     if world == 1 and not args.no_extras and args.workload == "1m":
         line["precision_form"] = run_precision_form(sc, args, opts)
     if world == 1 and not args.no_extras:
         line["batched"] = run_batched(args)
         line["serving"] = run_serve(args, tuple(line["batched"]["tiling"]))
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------- the reference's own GPU step -----
+def run_reference_gpu(sc, ours_ms_per_step: float, e2e: dict | None = None, steps: int = 10,
+                      warmup: int = 3) -> dict:
+    """Baseline (a): the reference's leap_frog::step (src/leap_frog.cu:121-195)
+    built for sm_100a from its own sources (baseline/build_ref_gpu.sh), on the
+    same scene and GPU, timed with CUDA events around its step loop (its step
+    synchronises the device after its launches; setup and read-back excluded)."""
+    from baseline import refgpu
+    variant = refgpu.variant_of(sc)
+    if variant is None or not refgpu.available(variant):
+        return {"unavailable": "the reference's GPU build (baseline/_ref) is not built here"}
+    rec = refgpu.run(sc, warmup, steps)
+    ms = rec["ms_per_step"]
+    out = {"metric": "particle-steps/s", "value": sc.n / (ms * 1e-3), "unit": "particle-steps/s",
+           "ms_per_step": ms, "steps": steps, "warmup": warmup, "variant": variant,
+           "ours_over_reference_device": ms / ours_ms_per_step,
+           "build": "the reference's sources, -O3 -rdc=true for sm_100a, texture references read through __ldg "
+                    "and a project-written GLM-compatible header (baseline/build_ref_gpu.sh)",
+           "timing": "CUDA events around the reference's step loop, after warm-up"}
+    if e2e and e2e.get("value"):
+        out["ours_e2e_over_reference_device"] = e2e["value"] / out["value"]
+    return out
+
+
+def run_grain(args, opts) -> dict:
+    """The single-grain configuration (4.1M particles, compensated positions):
+    particle-steps/s and HBM GB/s, timed like the main line, with the
+    reference's own GPU step on the same scene beside it."""
+    from iwf_mfree_gpu_3d_b200 import api
+    sc = make_scene("grain")
+    sim = api.Simulation.from_scene(sc, **opts)
+    sim.advance(max(args.warmup, 3), use_graph=True)
+    sim.sync()
+    steps = min(args.steps, 20)
+    sim.timer_start()
+    sim.advance(steps, use_graph=True)
+    ms = sim.timer_stop()
+    sim.close()
+    value = sc.n * steps / (ms * 1e-3)
+    out = {"metric": "particle-steps/s", "value": value, "ms_per_step": ms / steps, "steps": steps,
+           "config": workload_config("grain", sc), "hbm": hbm_roofline(value, sc),
+           "timing": "CUDA events around K graph replays, as the main line"}
+    if not args.no_reference_gpu:
+        out["reference_gpu"] = run_reference_gpu(sc, ms / steps, steps=5, warmup=2)
+    return out
 
 
 # ------------------------------------------------------ systems forms -----
@@ -485,23 +547,38 @@ def run_batched(args) -> dict:
 
 
 def run_serve(args, tiling) -> dict:
-    """Poisson request stream into one resident batch (continuous batching)."""
+    """Poisson request stream into one resident batch (continuous batching):
+    the serving configuration's arrival process (20 requests/s, scenes
+    log-uniform in [10k, 500k] particles), over a shorter arrival window and
+    with every request's step count scaled (both stated in the line)."""
     from iwf_mfree_gpu_3d_b200 import serve
-    lo, hi = args.serve_steps
+    lo, hi = int(round(500 * args.serve_step_scale)), int(round(5000 * args.serve_step_scale))
     reqs = serve.poisson_requests(rate=args.serve_rate, duration=args.serve_seconds, seed=2, n_lo=10000,
                                   n_hi=args.serve_nmax, steps_lo=lo, steps_hi=hi)
     srv = serve.Server(hbm_budget=150 * 10**9, chunk_steps=args.serve_chunk, tiling=tiling)
-    out = srv.run(reqs, horizon=4 * args.serve_seconds)
+    horizon = 4 * args.serve_seconds
+    out = srv.run(reqs, horizon=horizon)
     srv.close()
     offered = sum(r.spec.n * r.spec.steps for r in reqs) / args.serve_seconds
+    trace, last = [], -1e9
+    for t, waiting, running, parts in out["queue_trace"]:  # about one sample per 2 s
+        if t - last >= 2.0:
+            trace.append([round(t, 2), waiting, running, parts])
+            last = t
     return {"metric": "p50/p99 solve latency (s)", "p50_s": out["p50_s"], "p99_s": out["p99_s"],
+            "p50_with_censored_s": out["p50_censored_s"], "p99_with_censored_s": out["p99_censored_s"],
             "particle_steps_per_s": out["particle_steps_per_s"], "offered_particle_steps_per_s": offered,
             "requests": out["offered"], "completed": out["completed"], "unfinished": out["unfinished"],
-            "elapsed_s": out["elapsed_s"], "chunk_steps": args.serve_chunk, "budget_bytes": 150 * 10**9,
-            "timing": "wall clock on the host, arrival to result read-back",
+            "censored": out["censored"], "rejected": out["rejected"],
+            "elapsed_s": out["elapsed_s"], "horizon_s": horizon, "chunk_steps": args.serve_chunk,
+            "budget_bytes": 150 * 10**9,
+            "queue_trace": {"columns": ["t_s", "waiting", "running", "running_particles"], "rows": trace},
+            "timing": "wall clock on the host, arrival to result read-back; requests unfinished at the horizon "
+                      "enter the *_with_censored_s percentiles at the time they have waited (lower bounds)",
             "config": f"Poisson {args.serve_rate}/s for {args.serve_seconds} s (seed 2), n log-uniform "
-                      f"[10k, {args.serve_nmax}], steps U[{lo}, {hi}]: the serving configuration "
-                      "(20/s, 600 s, [10k, 500k], U[500, 5000]) scaled down to finish in seconds"}
+                      f"[10k, {args.serve_nmax}], steps U[{lo}, {hi}]: the serving configuration (20/s for "
+                      f"600 s, [10k, 500k], U[500, 5000]) with the arrival window shortened to "
+                      f"{args.serve_seconds:g} s and each request's step count scaled by {args.serve_step_scale:g}"}
 
 
 def run_e2e(sc, args, opts, dist, local_rank) -> dict:

@@ -120,6 +120,7 @@ class Server:
         t0 = clock()
         psteps = 0
         chunks = 0
+        queue_trace = []  # (time, requests arrived and waiting, requests running, running particles)
         while pending or waiting or active:
             now = clock() - t0
             if horizon is not None and now > horizon:
@@ -149,6 +150,8 @@ class Server:
                 if pending:
                     time.sleep(max(0.0, min(0.05, pending[0].arrival - (clock() - t0))))
                 continue
+            queue_trace.append((clock() - t0, len(waiting), len(active),
+                                sum(v[2].n_init for v in active.values())))
             # a chunk of steps (the batch stops each scene at its own count)
             before = {s: self.batch.query(s)[0] for s in active}
             self.batch.step(self.chunk, record_every=0, use_graph=self.use_graph)
@@ -169,6 +172,11 @@ class Server:
                                       admitted=t_adm, finished=finished, state=state))
         elapsed = clock() - t0
         lat = np.array([r.latency for r in results]) if results else np.zeros(0)
+        # requests still queued or running when the loop stops are censored: their
+        # latency is at least the time they have waited so far
+        unfinished = [v[0] for v in active.values()] + list(waiting) + [r for r in pending if r.arrival <= elapsed]
+        cens = np.array([elapsed - r.arrival for r in unfinished]) if unfinished else np.zeros(0)
+        both = np.concatenate([lat, cens])
         return dict(
             results=results,
             completed=len(results),
@@ -180,6 +188,12 @@ class Server:
             particle_steps_per_s=psteps / elapsed if elapsed > 0 else 0.0,
             p50_s=float(np.percentile(lat, 50)) if lat.size else None,
             p99_s=float(np.percentile(lat, 99)) if lat.size else None,
+            # p50/p99 over completed and censored requests, the censored ones at
+            # their lower bound (a lower bound of the true percentiles)
+            p50_censored_s=float(np.percentile(both, 50)) if both.size else None,
+            p99_censored_s=float(np.percentile(both, 99)) if both.size else None,
+            censored=int(cens.size),
+            queue_trace=queue_trace,
             chunks=chunks,
         )
 
