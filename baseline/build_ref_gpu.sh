@@ -57,6 +57,7 @@ for v in $variants; do
         *) echo "unknown variant $v" >&2; exit 1 ;;
     esac
     flags="-O3 -std=c++17 -rdc=true -gencode arch=compute_100a,code=sm_100a -w -include $here/ref_compat.h -I$root/oracle/ref_include -I$src"
+    # (ref_compat.h includes oracle/ref_include/ref_prelude.h)
     for u in $units; do echo "$src/$u"; done > "$tmp/$v/list"
     echo "$here/ref_step_main.cu" >> "$tmp/$v/list"
     # every unit is compiled (in parallel) before a failure is reported

@@ -10,28 +10,8 @@
 // variable, a fetch is a read-only-cache load of element i (what a linear
 // texture fetch returned), unbinding does nothing.  Element values are the same
 // as the texture path's, so the reference's arithmetic is unchanged.
-//
-// It also includes, before the reference's own headers, the standard and
-// Thrust headers whose content CUDA 8 brought in transitively (FLT_MAX,
-// DBL_MAX, thrust::count ...).  Included first, they are also read before
-// src/types.h defines float_t as a macro (types.h:69), which would otherwise
-// break the C++ library's own float_t in <cmath>.
 #pragma once
-#include <cfloat>
-#include <cmath>
-#include <cstdio>
-#include <cstdlib>
-#include <cassert>
-#include <vector>
-#include <cuda_runtime.h>
-#include <thrust/count.h>
-#include <thrust/device_ptr.h>
-#include <thrust/device_vector.h>
-#include <thrust/extrema.h>
-#include <thrust/functional.h>
-#include <thrust/reduce.h>
-#include <thrust/sequence.h>
-#include <thrust/sort.h>
+#include "ref_prelude.h"
 
 template <class T, int dim = 1, enum cudaTextureReadMode mode = cudaReadModeElementType>
 struct ref_texture {

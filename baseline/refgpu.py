@@ -56,6 +56,7 @@ def build(reference_root: Optional[str] = None, variants=VARIANTS) -> bool:
         return all(available(v) for v in variants)
     deps = [os.path.join(HERE, f) for f in ("build_ref_gpu.sh", "ref_compat.h", "ref_step_main.cu")]
     deps.append(os.path.join(os.path.dirname(HERE), "oracle", "ref_include", "glm", "glm.hpp"))
+    deps.append(os.path.join(os.path.dirname(HERE), "oracle", "ref_include", "ref_prelude.h"))
     newest = max(os.path.getmtime(d) for d in deps)
     stale = [v for v in variants if not available(v) or os.path.getmtime(binary(v)) < newest]
     if stale:

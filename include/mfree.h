@@ -454,6 +454,9 @@ int mfree_append_force_log(mfree_ctx *ctx, const char *path);
 int mfree_read_mesh_json(const char *path, float **verts, int *nv, int **tris, int *nt);
 /* ldynak_read_triangles_from_tetmesh (ldynak_reader.cpp:371-434): LS-DYNA .k */
 int mfree_read_mesh_ldynak(const char *path, float **verts, int *nv, int **tris, int *nt);
+/* ldynak_read_triangles_from_quadmesh (ldynak_reader.cpp:308-369): LS-DYNA .k of
+ * hexahedral solids; each boundary face gives two triangles */
+int mfree_read_mesh_ldynak_quad(const char *path, float **verts, int *nv, int **tris, int *nt);
 void mfree_free(void *p);
 
 #ifdef __cplusplus

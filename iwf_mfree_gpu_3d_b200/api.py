@@ -37,7 +37,7 @@ EXPORTS = [
     "mfree_get_tool_info", "mfree_get_tool_normals", "mfree_get_tool_cells", "mfree_step", "mfree_advance",
     "mfree_sync", "mfree_get_counts", "mfree_field_width", "mfree_get_field", "mfree_set_field",
     "mfree_get_field_f64", "mfree_get_cells", "mfree_get_grid", "mfree_get_counters", "mfree_read_mesh_json",
-    "mfree_read_mesh_ldynak", "mfree_free", "mfree_set_kernel_timing", "mfree_get_kernel_times",
+    "mfree_read_mesh_ldynak", "mfree_read_mesh_ldynak_quad", "mfree_free", "mfree_set_kernel_timing", "mfree_get_kernel_times",
     "mfree_probe_fp32_peak", "mfree_timer_start", "mfree_timer_stop", "mfree_set_device",
     "mfree_cell_list_static", "mfree_batch_create", "mfree_batch_destroy", "mfree_batch_admit", "mfree_batch_step",
     "mfree_batch_query", "mfree_batch_context", "mfree_batch_retire", "mfree_batch_info", "mfree_batch_set_tiling",
@@ -142,6 +142,7 @@ def lib(path: str = LIB_PATH):
     L.mfree_get_counters.argtypes = [P, C.POINTER(Counters)]
     L.mfree_read_mesh_json.argtypes = [C.c_char_p, C.POINTER(fp), ip, C.POINTER(ip), ip]
     L.mfree_read_mesh_ldynak.argtypes = [C.c_char_p, C.POINTER(fp), ip, C.POINTER(ip), ip]
+    L.mfree_read_mesh_ldynak_quad.argtypes = [C.c_char_p, C.POINTER(fp), ip, C.POINTER(ip), ip]
     L.mfree_free.argtypes = [P]
     L.mfree_set_kernel_timing.argtypes = [P, I]
     L.mfree_get_kernel_times.argtypes = [P, C.POINTER(C.c_double), ip]
@@ -204,14 +205,18 @@ def fp32_peak_tflops() -> float:
     return v.value
 
 
-def read_mesh(path: str):
-    """Read a MeshLab .json or LS-DYNA .k tool mesh: (verts (nv,3) float32, tris (nt,3) int32)."""
+def read_mesh(path: str, hexahedra: bool = False):
+    """Read a MeshLab .json or LS-DYNA .k tool mesh (tetrahedral solids, or
+    hexahedral ones with hexahedra=True): (verts (nv,3) float32, tris (nt,3) int32)."""
     L = lib()
     vp = C.POINTER(C.c_float)()
     tp = C.POINTER(C.c_int)()
     nv = C.c_int()
     nt = C.c_int()
-    fn = L.mfree_read_mesh_json if path.endswith(".json") else L.mfree_read_mesh_ldynak
+    if path.endswith(".json"):
+        fn = L.mfree_read_mesh_json
+    else:
+        fn = L.mfree_read_mesh_ldynak_quad if hexahedra else L.mfree_read_mesh_ldynak
     st = fn(path.encode(), C.byref(vp), C.byref(nv), C.byref(tp), C.byref(nt))
     if st != 0:
         raise MfreeError(st, f"could not read mesh {path}")

@@ -256,6 +256,31 @@ def two_tool_scene(nx: int = 40, ny: int = 20, nz: int = 10, dx: float = 1.0e-3,
     return sc
 
 
+def mesh_tool_scene(verts: np.ndarray, tris: np.ndarray, nx: int = 30, ny: int = 15, nz: int = 10,
+                    dx: float = 1.0e-3, v_tool: float = 1.0e-3, depth: float = 3.0, engage: float = 0.05,
+                    algorithm: int = 0, **kw) -> Scene:
+    """A steel block cut by a tool read from a mesh file (api.read_mesh), placed
+    the way the reference's single-grain setup places its LS-DYNA tool
+    (benchmarks_single_grain.cu:689-707): lifted so that its lowest point lies
+    depth*dx below the top surface, centred in y, and moved in x until its
+    far side overlaps the block's -x face by engage*dx; it moves towards +x at
+    v_tool.  Grid and blanking box cover block and tool, padded by 15*dx."""
+    sc = orthogonal_cutting(nx, ny, nz, dx, v_tool=v_tool, **kw)
+    v = np.asarray(verts, np.float64).copy()
+    lo, hi = v.min(0), v.max(0)
+    v[:, 2] += -lo[2] - depth * dx
+    v[:, 1] += -lo[1] - (hi[1] - lo[1]) / 2.0
+    v[:, 0] += -hi[0] + engage * dx
+    sc.tools = [Tool(verts=v.astype(np.float32), tris=np.asarray(tris, np.int32),
+                     vel=np.array([v_tool, 0.0, 0.0], np.float32), algorithm=algorithm)]
+    pad = 15.0 * dx
+    lo = (np.minimum(sc.pos[:, :3].min(0), v.min(0)) - pad).astype(np.float32)
+    hi = (np.maximum(sc.pos[:, :3].max(0), v.max(0)) + pad).astype(np.float32)
+    sc.grid_bbmin, sc.grid_bbmax, sc.blank_bbmin, sc.blank_bbmax = lo, hi, lo.copy(), hi.copy()
+    sc.name = f"mesh_tool_{nx}x{ny}x{nz}"
+    return sc
+
+
 def small_scene(**kw) -> Scene:
     """40 x 20 x 10 = 8,000 particles, Brookshaw, no CSPM (the 8k workload)."""
     return orthogonal_cutting(40, 20, 10, **kw)

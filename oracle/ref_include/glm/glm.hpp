@@ -16,7 +16,8 @@
 //  * m * v treats v as a column vector, v * m as a row vector, and m1 * m2 is
 //    the matrix product (column c of the result is m1 applied to column c of
 //    m2);
-//  * dot, cross, length = sqrt(dot(v, v)), normalize = v / length(v),
+//  * dot, cross, length = sqrt(dot(v, v)), normalize = v * (1 / sqrt(dot(v, v)))
+//    (GLM's normalize goes through its inversesqrt),
 //    transpose, determinant (cofactor expansion along the first row) and
 //    inverse (adjugate divided by the determinant).
 //
@@ -107,7 +108,11 @@ template <typename T> REFGLM_FN tvec3<T> cross(const tvec3<T> &a, const tvec3<T>
 }
 template <typename T> REFGLM_FN T length(const tvec3<T> &a) { using std::sqrt; return sqrt(dot(a, a)); }
 template <typename T> REFGLM_FN T length(const tvec2<T> &a) { using std::sqrt; return sqrt(dot(a, a)); }
-template <typename T> REFGLM_FN tvec3<T> normalize(const tvec3<T> &a) { return a / length(a); }
+// GLM normalizes through its inverse square root, 1 / sqrt(x): v * (1 / |v|)
+template <typename T> REFGLM_FN tvec3<T> normalize(const tvec3<T> &a) {
+    using std::sqrt;
+    return a * (T(1) / sqrt(dot(a, a)));
+}
 
 // ------------------------------------------------------------- mat3x3 --
 template <typename T>

@@ -31,6 +31,9 @@ TOL = {
     # exhaustive contact, 30 steps (8.8e-5, 2.6e-5, 1.8e-5, 2.1e-5, 2.2e-5, 1.5e-7;
     # the reference's own GPU step measures the same against this oracle)
     "exhaustive_30": dict(POS=2.7e-4, VEL=8e-5, S=5.4e-5, EPS_PL=6.3e-5, T=6.8e-5, RHO=4.5e-7),
+    # a 30x15x10 block cut by the reference's pin25 grain mesh, 100 steps
+    # (2.4e-5, 4.5e-5, 3.9e-5, 4.5e-7, 7.8e-7, 1.3e-7)
+    "pin25_100": dict(POS=7.2e-5, VEL=1.4e-4, S=1.2e-4, EPS_PL=1.4e-6, T=2.3e-6, RHO=4e-7),
     # two wedges, 100 steps (2.4e-5, 2.5e-5, 3.2e-5, 5.0e-6, 7.7e-6, 2.2e-7, contact 9.8e-5)
     "two_tools_100": dict(POS=7e-5, VEL=8e-5, S=1e-4, EPS_PL=1.5e-5, T=2.3e-5, RHO=6.5e-7, FC=3e-4),
     # tool particles conducting heat, 40 steps: only the tool particles move, by
@@ -145,3 +148,32 @@ def loaded(sc, seed: int = 7):
     sc.T = (300.0 + rng.uniform(0.0, 200.0, n)).astype(np.float32)
     sc.rho = (sc.rho * (1.0 + rng.normal(0.0, 1e-3, n))).astype(np.float32)
     return sc
+
+
+def hex_block_k(nx: int = 3, ny: int = 2, nz: int = 2, seed: int = 11) -> str:
+    """An LS-DYNA keyword file of an nx x ny x nz block of hexahedral solids
+    (*NODE, *ELEMENT_SOLID with eight node ids), node ids shuffled and
+    coordinates jittered, for the hexahedral-mesh reader."""
+    rng = np.random.default_rng(seed)
+    npts = (nx + 1) * (ny + 1) * (nz + 1)
+    ids = rng.permutation(npts) + 1
+    def nid(i, j, k):
+        return int(ids[(i * (ny + 1) + j) * (nz + 1) + k])
+    lines = ["*KEYWORD", "*NODE", "$#   nid               x               y               z      tc      rc"]
+    order = rng.permutation(npts)
+    for o in order:
+        i, rem = divmod(int(o), (ny + 1) * (nz + 1))
+        j, k = divmod(rem, nz + 1)
+        x, y, z = np.array([i, j, k], float) * 1e-3 + rng.uniform(-1e-5, 1e-5, 3)
+        lines.append(f"{nid(i, j, k):10d} {x:.9g} {y:.9g} {z:.9g} 0 0")
+    lines += ["*ELEMENT_SOLID", "$#   eid     pid      n1      n2      n3      n4      n5      n6      n7      n8"]
+    e = 1
+    for i in range(nx):
+        for j in range(ny):
+            for k in range(nz):
+                n = [nid(i, j, k), nid(i + 1, j, k), nid(i + 1, j + 1, k), nid(i, j + 1, k),
+                     nid(i, j, k + 1), nid(i + 1, j, k + 1), nid(i + 1, j + 1, k + 1), nid(i, j + 1, k + 1)]
+                lines.append(f"{e:8d}{1:8d}" + "".join(f"{v:8d}" for v in n))
+                e += 1
+    lines.append("*END")
+    return "\n".join(lines) + "\n"
