@@ -373,12 +373,20 @@ def single_grain(nx: int = 400, ny: int = 160, nz: int = 64, dx: float = 1.0e-3,
     sc = orthogonal_cutting(nx, ny, nz, dx=dx, v_tool=v_tool, depth=depth, seed=seed,
                             precision=precision, name=f"grain_{nx}x{ny}x{nz}")
     R = radius * dx
-    v, f = truncated_grain(R)
+    rake, cut = -10.0, 0.5
+    v, f = truncated_grain(R, rake_deg=rake, cut=cut)
     lx = (nx - 1) * dx
-    # place the flattened face on the +x face, its lowest point depth*dx below the top
+    # lowest point depth*dx below the top surface; the flattened face, where it
+    # crosses the top surface (its foremost point inside the block: the face
+    # leans by the rake angle), overlaps the +x face by engage*dx, so the grain
+    # is in contact from the first step
     v = v.copy()
-    v[:, 0] += lx - engage * dx - v[:, 0].min()
-    v[:, 2] += -depth * dx - v[:, 2].min()
+    tz = -depth * dx - v[:, 2].min()
+    a = math.radians(rake)
+    nxp, nzp = -math.cos(a), math.sin(a)          # the face's outward normal (x, z); n . p = cut * R
+    x_face = (cut * R - nzp * (-tz)) / nxp        # the face's x at local z = -tz (world z = 0)
+    v[:, 0] += lx - engage * dx - x_face
+    v[:, 2] += tz
     sc.tools = [Tool(verts=v.astype(np.float32), tris=f, vel=np.array([-v_tool, 0, 0], np.float32))]
     if tool_particles:
         lo, hi = v.min(0), v.max(0)

@@ -40,8 +40,20 @@ TOL = {
     # a rigid translation of ~4e-4 dx per step that FP32 rounds at every step
     # (displacement 3.4e-3; T 4.5e-5)
     "tool_particles_40": dict(POS=1e-2, T=1.4e-4),
-    # single grain with tool particles, 40 steps (3.3e-6, 4.6e-6, 1.1e-4, 1.1e-6, 2.8e-6, 1.7e-7)
-    "grain_40": dict(POS=1e-5, VEL=1.4e-5, S=3.4e-4, EPS_PL=3.4e-6, T=8.5e-6, RHO=5.1e-7),
+    # single grain with tool particles, 40 steps, in contact from the first
+    # step.  The reference's inside test counts a +z ray's hit only in the grid
+    # cell that holds it, and on this 1,280-triangle mesh a hit can fall in a
+    # cell where its triangle is not registered: such a particle is taken for
+    # inside and pushed hard (tool_3d_gpu.cu:382-444).  Which particles, depends
+    # on last bits, so FP32 and FP64 part within a few steps: the reference's
+    # own FP32 GPU step measures 5.0e-2, 8.6e-2, 4.4e-2, 8.1e-3, 2.3e-2, 1.3e-3
+    # against the FP64 oracle, and so does this path.  These bounds serve
+    # where the reference's GPU build is not at hand (grain_vs_ref below).
+    "grain_40": dict(POS=0.15, VEL=0.26, S=0.13, EPS_PL=2.4e-2, T=6.8e-2, RHO=4e-3),
+    # the CUDA path (plain FP32) against the reference's own GPU step on the
+    # grain scenes (measured 40 steps small: 2.3e-6, 4.6e-6, 3.0e-5, 7.5e-7,
+    # 1.3e-6, 1.5e-7; 10 steps full size: ~1e-7)
+    "grain_vs_ref": dict(POS=2e-5, VEL=4e-5, S=2e-4, EPS_PL=6e-6, T=1e-5, RHO=1e-6),
     # a served request after 100 steps (4.2e-6, 2.1e-5, 1.3e-5, 4.1e-6, 1.5e-5, 1.2e-7)
     "served_100": dict(POS=1.3e-5, VEL=6.3e-5, S=3.9e-5, EPS_PL=1.3e-5, T=4.5e-5, RHO=3.6e-7),
     # the bounds-checked build, 30 steps, worst of its four variant families
@@ -177,3 +189,25 @@ def hex_block_k(nx: int = 3, ny: int = 2, nz: int = 2, seed: int = 11) -> str:
                 e += 1
     lines.append("*END")
     return "\n".join(lines) + "\n"
+
+
+def grain_checks(sc_plain, sim_plain, err_vs_fp64: dict, orc_state: dict, steps: int, fallback: str):
+    """The grain scenes' parity: the CUDA path (plain FP32) against the
+    reference's own GPU step, and the error against the FP64 oracle no larger
+    than the reference's own (10 % slack) -- or, without the reference's GPU
+    build, the fallback bounds."""
+    from baseline import refgpu
+    names = ["POS", "VEL", "S", "EPS_PL", "T", "RHO"]
+    if not refgpu.available(refgpu.variant_of(sc_plain)):
+        check(err_vs_fp64, fallback)
+        return
+    st = refgpu.run(sc_plain, 0, steps, state=True)["state"]
+    r = {n: by_id(st["ID"], st[n].astype(np.float64)) for n in names + ["BLANKED"]}
+    e_ref = compare(r, orc_state, sc_plain, names)
+    e_cuda = compare(gpu_state(sim_plain, names), r, sc_plain, names)
+    print("reference GPU step vs FP64 oracle:", {k: f"{v:.2e}" for k, v in e_ref.items()})
+    print("CUDA path (FP32) vs reference GPU step:", {k: f"{v:.2e}" for k, v in e_cuda.items()})
+    check(e_cuda, "grain_vs_ref")
+    assert err_vs_fp64["blank_mismatch"] == 0
+    for f in names:
+        assert err_vs_fp64[f] <= 1.1 * e_ref[f] + 1e-7, (f, err_vs_fp64[f], e_ref[f])

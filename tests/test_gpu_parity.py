@@ -11,7 +11,7 @@ import pytest
 import oracle
 from iwf_mfree_gpu_3d_b200 import api, scenes
 
-from helpers import check, compare, gpu_state, oracle_state
+from helpers import grain_checks, check, compare, gpu_state, oracle_state
 
 pytestmark = pytest.mark.gpu
 
@@ -117,6 +117,32 @@ def test_100_steps_against_fp64_oracle_full_size_1m_plain_and_precision():
     assert e_prec["POS"] <= 0.1 * e_plain["POS"]
     plain.close()
     prec.close()
+
+
+def test_single_grain_full_size_against_fp64_oracle():
+    """The single-grain configuration at full size: a 400 x 160 x 64 block
+    (4,096,000 particles) plus the grain's diamond tool particles, cut by the
+    1,280-triangle truncated icosphere at 30 m/s from the first step, 10 steps.
+    The compensated form (the configuration's form) against the FP64 oracle:
+    its per-field report is printed and is no larger than the reference's own
+    GPU step's; the plain FP32 form against the reference's GPU step."""
+    sc = scenes.single_grain()
+    sim = _sim(sc)
+    orc = oracle.Oracle(sc, prec=64)
+    for _ in range(10):
+        sim.step()
+        orc.step()
+    o = oracle_state(orc)
+    err = compare(gpu_state(sim, f64=True), o, sc)
+    sim.close()
+    print("single grain, 4.1M particles, 10-step relative L2 vs FP64 oracle: " +
+          ", ".join(f"{k} {v:.3e}" for k, v in err.items()))
+    sc0 = scenes.single_grain(precision=0)
+    plain = _sim(sc0)
+    for _ in range(10):
+        plain.step()
+    grain_checks(sc0, plain, err, o, 10, "grain_40")
+    plain.close()
 
 
 def test_one_step_against_fp32_oracle():
