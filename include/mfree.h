@@ -76,9 +76,12 @@ typedef struct {
     int tile_depth;         /* pair-loop tiling: cells per tile along z, 1..8; 0 picks
                                the tuned default (6).  Results do not depend on it.   */
     int full_stencil;       /* 1: the pair loop visits every candidate of the 5x5x5
-                               cell stencil.  0 (default): without PSE conduction it
-                               skips the stencil cells that lie wholly beyond the
-                               target's support radius.  Results do not depend on it. */
+                               cell stencil and evaluates every term.  0 (default):
+                               it skips the stencil cells that lie wholly beyond the
+                               target's support radius -- with PSE conduction only on
+                               tiles whose PSE sums are exactly zero (every
+                               temperature their stencils reach equal), where it also
+                               skips the PSE terms.  Results do not depend on it.     */
 } mfree_options;
 
 /* ---- fields for mfree_get_field / mfree_set_field ------------------------
@@ -155,6 +158,11 @@ typedef struct {
                                    predictor (variants without PSE; see full_stencil) */
     int64_t bounds_errors;      /* bounds-checked library only: data-derived indices
                                    that fell outside their array (always 0 otherwise) */
+    int64_t pse_zero_targets;   /* PSE conduction: targets whose PSE sum was exactly zero
+                                   because every temperature their tile's stencils reach
+                                   was equal (with finite positions and volumes); the
+                                   pair loop skipped the PSE terms and pruned the stencil
+                                   for them, with the same results, summed over steps */
 } mfree_counters;
 
 typedef struct mfree_ctx mfree_ctx;

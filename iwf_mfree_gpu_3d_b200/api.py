@@ -86,7 +86,7 @@ class Options(C.Structure):
 class Counters(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("steps", "secant_failures", "out_of_grid", "contact_search_cap",
                                          "nan_blanked", "staging_timeouts", "full_stencil_steps",
-                                         "bounds_errors")]
+                                         "bounds_errors", "pse_zero_targets")]
 
 
 _lib = None

@@ -57,6 +57,8 @@ struct DevClock {
     // device-detected conditions (mfree_counters)
     unsigned long long secant_failures, out_of_grid, contact_cap, nan_blanked, full_stencil_steps;
     unsigned long long bounds_errors;  // bounds-checked builds: indices from data that fell outside their array
+    unsigned long long pse_zero_targets;  // PSE variants: targets of tiles whose PSE sum is exactly zero (all
+                                          // staged temperatures equal), run without the PSE terms
 };
 
 // Bounds-checked build (-DMFREE_BOUNDS_CHECK, libmfree_checked.so): every

@@ -1094,6 +1094,7 @@ int mfree_get_counters(mfree_ctx *c, mfree_counters *o) {
     o->staging_timeouts = int64_t(h.staging_timeouts);
     o->full_stencil_steps = int64_t(h.full_stencil_steps);
     o->bounds_errors = int64_t(h.bounds_errors);
+    o->pse_zero_targets = int64_t(h.pse_zero_targets);
     return MFREE_OK;
 }
 

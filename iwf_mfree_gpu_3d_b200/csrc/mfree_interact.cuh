@@ -898,7 +898,7 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
         const int gstride = a.p.n_init;
         const int ntg = sm.tpref[NTC];
         const bool staged = sm.staged != 0;
-        if (COND != MFREE_COND_PSE && threadIdx.x == 0) {  // read by the targets after the next barrier
+        if (threadIdx.x == 0) {  // read by the targets after the next barrier
             float4 org = make_float4(0.f, 0.f, 0.f, 0.f);
             const float md = __uint_as_float(a.clk->max_disp);
             if (!a.p.full_stencil && md <= PRUNE_DISP_MAX) {
@@ -930,6 +930,23 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
             }
             if (threadIdx.x == 0) sm.parity ^= 1;
         }
+        // PSE: every term carries T_j - T_i, so when all staged records of the
+        // tile hold the same temperature (and finite positions and volumes)
+        // each term is exactly +0 and so is every target's sum; such a tile runs
+        // the variant without conduction terms, on the pruned stencil, with the
+        // same results.  The test reads the staged halo after the wait.
+        bool pse_zero = false;
+        if (COND == MFREE_COND_PSE && staged && sm.total > 0 && !a.p.full_stencil) {
+            const float4 *rc = sarr + REC_C * CAP, *rp = sarr + REC_P * CAP;
+            const float T0 = rc[0].z;
+            bool u = true;
+            for (int k = threadIdx.x; k < sm.total; k += TILE_THREADS) {
+                const float4 c = rc[k], p = rp[k];
+                u = u && c.z == T0 && isfinite(c.w) && isfinite(p.x) && isfinite(p.y) && isfinite(p.z);
+            }
+            pse_zero = __syncthreads_and(u) != 0;
+            if (pse_zero && threadIdx.x == 0) atomicAdd(&a.clk->pse_zero_targets, (unsigned long long)ntg);
+        }
         for (int t0 = 0; t0 < ntg; t0 += TCAP) {
             const int tn = min(TCAP, ntg - t0);
             const bool last = t0 + TCAP >= ntg;
@@ -958,7 +975,10 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
                     const int tt = done + warp;
                     const bool valid = tt < tn;
                     const int i = sm.tgt[valid ? tt : 0];
-                    if (staged)
+                    if (staged && COND == MFREE_COND_PSE && pse_zero)
+                        process_target<32, CSPM, MFREE_COND_NONE, true>(a, sm, sarr, CAP, i, valid, tt, warp, 0, lane, lane, X0,
+                                                             Y0, zl);
+                    else if (staged)
                         process_target<32, CSPM, COND, true>(a, sm, sarr, CAP, i, valid, tt, warp, 0, lane, lane, X0,
                                                              Y0, zl);
                     else
@@ -970,7 +990,10 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
                     const int tt = done + warp * 2 + g2;
                     const bool valid = tt < tn;
                     const int i = sm.tgt[valid ? tt : 0];
-                    if (staged)
+                    if (staged && COND == MFREE_COND_PSE && pse_zero)
+                        process_target<16, CSPM, MFREE_COND_NONE, true>(a, sm, sarr, CAP, i, valid, tt, warp, g2, sl2, lane, X0,
+                                                             Y0, zl);
+                    else if (staged)
                         process_target<16, CSPM, COND, true>(a, sm, sarr, CAP, i, valid, tt, warp, g2, sl2, lane, X0,
                                                              Y0, zl);
                     else
@@ -981,7 +1004,10 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
                     const int tt = done + warp * G + g;
                     const bool valid = tt < tn;
                     const int i = sm.tgt[valid ? tt : 0];
-                    if (staged)
+                    if (staged && COND == MFREE_COND_PSE && pse_zero)
+                        process_target<LPP, CSPM, MFREE_COND_NONE, true>(a, sm, sarr, CAP, i, valid, tt, warp, g, sl, lane, X0,
+                                                              Y0, zl);
+                    else if (staged)
                         process_target<LPP, CSPM, COND, true>(a, sm, sarr, CAP, i, valid, tt, warp, g, sl, lane, X0,
                                                               Y0, zl);
                     else

@@ -1,9 +1,11 @@
-"""Stencil pruning of the pair loop (variants without PSE conduction): the
-pair kernel skips the cells of the 5x5x5 stencil that lie wholly beyond the
-target's support radius.  Only out-of-support candidates are skipped, in the
-same order, so every field must equal the full-stencil run bit for bit; a
-step whose predictor moves a particle too far for the pruning's margin falls
-back to the full stencil and is counted."""
+"""Stencil pruning of the pair loop: the pair kernel skips the cells of the
+5x5x5 stencil that lie wholly beyond the target's support radius.  Only
+out-of-support candidates are skipped, in the same order, so every field must
+equal the full-stencil run bit for bit; a step whose predictor moves a
+particle too far for the pruning's margin falls back to the full stencil and
+is counted.  With PSE conduction, which sums every candidate of the stencil,
+only tiles whose PSE sums are exactly zero (every staged temperature equal)
+are pruned, and their PSE terms skipped -- again bit for bit."""
 import numpy as np
 import pytest
 
@@ -40,6 +42,33 @@ def test_pruned_stencil_equals_full_stencil(cspm, conduction):
     _assert_identical(fa, fb)
     assert ca["full_stencil_steps"] == 0
     assert cb["full_stencil_steps"] == 0
+
+
+@pytest.mark.parametrize("cspm", [True, False])
+def test_zero_pse_tiles_equal_the_full_evaluation(cspm):
+    """PSE conduction from a uniform temperature: every tile starts with
+    exactly-zero PSE sums and is run without them on the pruned stencil;
+    plastic work and friction heat the particles at the tool, whose tiles then
+    evaluate the PSE terms.  60 steps, bit for bit against the full
+    evaluation, with both kinds of tile counted."""
+    sc = scenes.orthogonal_cutting(30, 15, 12, cspm=cspm, conduction=2)
+    (fa, ca), (fb, cb) = _pair(sc, 60)
+    _assert_identical(fa, fb)
+    n = sc.n
+    assert cb["pse_zero_targets"] == 0
+    assert ca["pse_zero_targets"] >= n  # the first step: every tile
+    assert ca["pse_zero_targets"] < 60 * n  # heated tiles evaluated the PSE terms
+    assert not np.all(fa["T"] == fa["T"][0])
+
+
+def test_zero_pse_skip_leaves_nonuniform_temperatures_alone():
+    """A random temperature field: no tile has a zero PSE sum, and the fields
+    equal the full evaluation."""
+    sc = scenes.orthogonal_cutting(30, 15, 12, cspm=True, conduction=2)
+    sc.T = (300.0 + np.random.default_rng(3).uniform(0.0, 50.0, sc.n)).astype(np.float32)
+    (fa, ca), (fb, _) = _pair(sc, 5)
+    _assert_identical(fa, fb)
+    assert ca["pse_zero_targets"] == 0
 
 
 def _kick(speed):
