@@ -92,7 +92,10 @@ __device__ __forceinline__ void hash_body(const StepArgs &a, int bid) {
                       p.y <= c->blank_max[1] && p.z >= c->blank_min[2] && p.z <= c->blank_max[2];
             if (fast || !in) {
                 blanked = 1.f;
-            } else {
+            } else if (blanked != 0.f) {
+                // inside and slow: the reference unblanks unless a rate is NaN/Inf
+                // (actions_gpu.cu:504-529), and a particle that is not blanked
+                // stays so either way -- the rates are read only to unblank
                 float4 da = a.a.da4[i], dv = a.a.dv4[i], dsa = a.a.dsa4[i], dsb = a.a.dsb4[i];
                 bool bad = nan_or_inf(da.x) || nan_or_inf(da.y) || nan_or_inf(da.z) || nan_or_inf(dv.x) ||
                            nan_or_inf(dv.y) || nan_or_inf(dv.z) || nan_or_inf(dsa.x) || nan_or_inf(dsa.y) ||
