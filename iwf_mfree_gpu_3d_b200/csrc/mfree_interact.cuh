@@ -56,11 +56,12 @@ __device__ __forceinline__ void inv3s(const float *m, float det, float *o) {
     o[5] = (m[3] * m[4] - m[0] * m[5]) * id;  // yz
 }
 
+// the target's terms of the pair loop; its own sigma and R enter the stress
+// divergence only through the group's sums (see pair_body) and are read after
+// the loop
 struct IData {
     float x, y, z, vx, vy, vz, rho, c, h, T, tool;
     float h1, fac;
-    float s[6];  // sigma_i xx yy zz xy xz yz
-    float R[6];  // R_i
 };
 
 // gradient factor of cubic_spline (kernels.cuh:26-69): value w and
@@ -106,20 +107,20 @@ __device__ __forceinline__ void pair_body(const Params &P, const IData &I, const
         acc[0] = fmaf(ax, gx, acc[0]); acc[1] = fmaf(ax, gy, acc[1]); acc[2] = fmaf(ax, gz, acc[2]);
         acc[3] = fmaf(ay, gx, acc[3]); acc[4] = fmaf(ay, gy, acc[4]); acc[5] = fmaf(ay, gz, acc[5]);
         acc[6] = fmaf(az, gx, acc[6]); acc[7] = fmaf(az, gy, acc[7]); acc[8] = fmaf(az, gz, acc[8]);
-        float Rxx = 0.f, Ryy = 0.f, Rzz = 0.f, Rxy = 0.f, Rxz = 0.f, Ryz = 0.f;
+        // sum_j (sigma_i + sigma_j + fab (R_i + R_j)) g
+        //   = sum_j (sigma_j + fab R_j) g + sigma_i sum_j g + R_i sum_j fab g:
+        // slots 19-21 and 22-24 hold sum_j g and sum_j fab g, which the caller
+        // multiplies by the target's sigma and R once
+        float txx = Aj.x, tyy = Aj.y, tzz = Aj.z, txy = Aj.w, txz = Bj.x, tyz = Bj.y;
         if (P.wdeltap > 0.f) {
             float fab = w * P.inv_wdeltap;
             fab *= fab;
             fab *= fab;
-            Rxx = fab * (I.R[0] + Rj.x);
-            Ryy = fab * (I.R[1] + Rj.y);
-            Rzz = fab * (I.R[2] + Rj.z);
-            Rxy = fab * (I.R[3] + Rj.w);
-            Rxz = fab * (I.R[4] + Cj.x);
-            Ryz = fab * (I.R[5] + Cj.y);
+            txx = fmaf(fab, Rj.x, txx); tyy = fmaf(fab, Rj.y, tyy); tzz = fmaf(fab, Rj.z, tzz);
+            txy = fmaf(fab, Rj.w, txy); txz = fmaf(fab, Cj.x, txz); tyz = fmaf(fab, Cj.y, tyz);
+            acc[22] = fmaf(fab, gx, acc[22]); acc[23] = fmaf(fab, gy, acc[23]); acc[24] = fmaf(fab, gz, acc[24]);
         }
-        const float txx = I.s[0] + Aj.x + Rxx, tyy = I.s[1] + Aj.y + Ryy, tzz = I.s[2] + Aj.z + Rzz;
-        const float txy = I.s[3] + Aj.w + Rxy, txz = I.s[4] + Bj.x + Rxz, tyz = I.s[5] + Bj.y + Ryz;
+        acc[19] += gx; acc[20] += gy; acc[21] += gz;
         acc[9] = fmaf(txx, gx, fmaf(txy, gy, fmaf(txz, gz, acc[9])));
         acc[10] = fmaf(txy, gx, fmaf(tyy, gy, fmaf(tyz, gz, acc[10])));
         acc[11] = fmaf(txz, gx, fmaf(tyz, gy, fmaf(tzz, gz, acc[11])));
@@ -404,19 +405,17 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
     const int tcell = sm.tcell[valid ? tt : 0];
     const int gi = X0 + (tcell >> 16) / TY, gj = Y0 + (tcell >> 16) % TY, gk = tcell & 0xffff;
     IData I;
+    int si = i;  // the target's own record
+    if (STAGED) {
+        const int lc = (gi - X0 + 2) * HY + (gj - Y0 + 2);
+        si = sm.hoff[lc] + (i - sm.hstart[lc]);
+        if (!bounds_ok(a.clk, si, rstride)) si = 0;
+    }
     {
-        int si = i;
-        if (STAGED) {
-            const int lc = (gi - X0 + 2) * HY + (gj - Y0 + 2);
-            si = sm.hoff[lc] + (i - sm.hstart[lc]);
-            if (!bounds_ok(a.clk, si, rstride)) si = 0;
-        }
-        const float4 Pi = rP[si], Vi = rV[si], Ai = rA[si], Bi = rB[si], Ri = rR[si], Ci = rC[si];
+        const float4 Pi = rP[si], Vi = rV[si], Bi = rB[si], Ci = rC[si];
         I.x = Pi.x; I.y = Pi.y; I.z = Pi.z; I.tool = Pi.w;
         I.vx = Vi.x; I.vy = Vi.y; I.vz = Vi.z; I.rho = Vi.w;
-        I.s[0] = Ai.x; I.s[1] = Ai.y; I.s[2] = Ai.z; I.s[3] = Ai.w; I.s[4] = Bi.x; I.s[5] = Bi.y;
         I.c = Bi.z; I.h = Bi.w;
-        I.R[0] = Ri.x; I.R[1] = Ri.y; I.R[2] = Ri.z; I.R[3] = Ri.w; I.R[4] = Ci.x; I.R[5] = Ci.y;
         I.T = Ci.z;
         I.h1 = 1.0f / I.h;
         I.fac = 0.31830988618379067f * I.h1 * I.h1 * I.h1;
@@ -661,15 +660,24 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
         if (det > 9.99999994e-9f) inv3s(Bm, det, invB);
     }
     // ---- pair body over the in-support neighbours
-    float acc[19];
+    float acc[25];
 #pragma unroll
-    for (int k = 0; k < 19; k++) acc[k] = 0.f;
+    for (int k = 0; k < 25; k++) acc[k] = 0.f;
     auto pterm = [&](int j) { pair_body<CSPM, COND>(P, I, invB, rP[j], rV[j], rA[j], rB[j], rR[j], rC[j], acc); };
     for (int q0 = 0; q0 < maxq; q0 += LPP) {
         const int q = q0 + sl;
         if (q < qv) pterm(qq[q]);
     }
     if (overflow) for_overflow(pterm);
+    {   // the target's own sigma and R: sigma_i sum g + R_i sum fab g, in each lane
+        const float4 Ai = rA[si], Bi = rB[si], Ri = rR[si], Ci = rC[si];
+        acc[9] = fmaf(Ai.x, acc[19], fmaf(Ai.w, acc[20], fmaf(Bi.x, acc[21], acc[9])));
+        acc[10] = fmaf(Ai.w, acc[19], fmaf(Ai.y, acc[20], fmaf(Bi.y, acc[21], acc[10])));
+        acc[11] = fmaf(Bi.x, acc[19], fmaf(Bi.y, acc[20], fmaf(Ai.z, acc[21], acc[11])));
+        acc[9] = fmaf(Ri.x, acc[22], fmaf(Ri.w, acc[23], fmaf(Ci.x, acc[24], acc[9])));
+        acc[10] = fmaf(Ri.w, acc[22], fmaf(Ri.y, acc[23], fmaf(Ci.y, acc[24], acc[10])));
+        acc[11] = fmaf(Ci.x, acc[22], fmaf(Ci.y, acc[23], fmaf(Ri.z, acc[24], acc[11])));
+    }
     constexpr int NACC = COND == MFREE_COND_PSE ? 18 : 19;  // (slot 18 holds the PSE sum already)
 #pragma unroll
     for (int o = LPP / 2; o >= 1; o >>= 1) {
