@@ -710,33 +710,32 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // builds its halo cell starts, its target ranges (read from the halo table:
 // the target columns are halo columns) and halo offsets, and issues its
 // staging copies.  The prepared tile is left in sm.tile / sm.scene (scene < 0:
-// none left).  Each call claims the list entry of the next call at its start
-// and, once it has issued its copies, starts fetching that entry into shared
-// memory, so neither the claim's round trip nor the entry's load waits in the
-// next call.  The caller guarantees that nothing reads the staged records or
-// the tile tables any more.  Kept out of line: inlined into the kernel's loop
-// it made the pair rounds about 7% slower (measured on the 1M-particle step).
+// none left).  Once its copies are issued, each call claims the list entry of
+// the next call and starts fetching it into shared memory: the claim's round
+// trip then overlaps the copies, and neither it nor the entry's load waits in
+// the next call (a global atomic still in flight holds up the barrier that
+// follows it until it is performed).  The target table and the halo table are
+// built by two warps at once, the halo table with one scan (lane l owns halo
+// columns 2l and 2l + 1; the staged order of the columns is free).  The caller
+// guarantees that nothing reads the staged records or the tile tables any
+// more.  Kept out of line: inlined into the kernel's loop it made the pair
+// rounds about 7% slower (measured on the 1M-particle step).
 template <int LPP, int W, int CAP>
 __device__ __noinline__ void prepare_tile(const BatchTable &T, TileSmem<LPP, W> &sm, StepArgs *sa, float4 *sarr,
                                           int busy_scene) {
     constexpr int PT = W * 32 - PRO_FIRST;
     const int ptid = threadIdx.x - PRO_FIRST, pl = ptid & 31, pw = ptid >> 5;
-    int pend = -1;  // (thread 0 of the prologue) list index claimed by this call
     for (;;) {
         if (ptid == 0) {
-            const int n = sm.list_n;
             int2 e = make_int2(0, -1);
-            if (pend >= 0) {  // after an empty entry (none are listed; kept for safety)
-                if (pend < n) e = T.tile_list[pend];
-            } else if (sm.pre_ok) {
+            if (sm.pre_ok) {
                 cp_async_wait_all();
                 e = sm.pre_entry;
-            } else {
+            } else {  // the first call, or after an empty entry (none are listed; kept for safety)
                 const int k = atomicAdd(T.tile_next, 1);
-                if (k < n) e = T.tile_list[k];
+                if (k < sm.list_n) e = T.tile_list[k];
             }
             sm.pre_ok = 0;
-            pend = e.y >= 0 ? atomicAdd(T.tile_next, 1) : n;  // not waited for until the end
             sm.ntile = e.x;
             sm.nscene = e.y;
         }
@@ -785,8 +784,7 @@ __device__ __noinline__ void prepare_tile(const BatchTable &T, TileSmem<LPP, W> 
         pro_sync(PT);
         if (pw == 0) {
             // target column ranges (cells Z0 .. Z0 + depth - 1 of the 16
-            // target columns), then, for a non-empty tile, the prefix sum of
-            // the 64 halo columns and the staging decision
+            // target columns) and their prefix
             int len = 0;
             if (pl < NTC) {
                 const int cx = G.X0 + pl / TY, cy = G.Y0 + pl % TY;
@@ -801,33 +799,43 @@ __device__ __noinline__ void prepare_tile(const BatchTable &T, TileSmem<LPP, W> 
             const int ti = group_scan<32>(len, pl);
             if (pl < NTC) sm.tpref[pl] = ti - len;
             if (pl == 31) sm.tpref[NTC] = ti;
-            if (__shfl_sync(0xffffffffu, ti, 31) > 0) {
-                int len2[2];
+        } else if (pw == 1) {
+            // the 64 halo columns (lane pl: columns 2 pl and 2 pl + 1), their
+            // staged offsets and the staging decision; the tile's target count
+            // (the same ranges as warp 0's) decides whether copies follow
+            int ntg = 0;
+            if (pl < NTC) {
+                const int cx = G.X0 + pl / TY, cy = G.Y0 + pl % TY;
+                if (cx < nx && cy < ny && G.Z0 < nz) {
+                    const int lc = (pl / TY + 2) * HY + (pl % TY + 2);
+                    ntg = sm.cellstart[lc][min(G.Z0 + P.tile_z - 1, nz - 1) + 1 - G.zl] -
+                          sm.cellstart[lc][G.Z0 - G.zl];
+                }
+            }
+            ntg = __reduce_add_sync(0xffffffffu, ntg);
+            int len2[2];
 #pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    const int c = pl + 32 * h;
-                    const int cx = G.X0 - 2 + c / HY, cy = G.Y0 - 2 + c % HY;
-                    const bool in = cx >= 0 && cx < nx && cy >= 0 && cy < ny;
-                    len2[h] = in ? sm.cellstart[c][G.nzr - 1] - sm.cellstart[c][0] : 0;
-                    sm.hstart[c] = sm.cellstart[c][0];
-                    // bounds-checked build: a column whose range lies outside
-                    // the record arrays is counted and not staged (len 0)
-                    if (!range_ok(a.clk, sm.hstart[c], len2[h], P.n_init)) len2[h] = 0;
-                    sm.hlen[c] = len2[h];
-                }
-                const int i0 = group_scan<32>(len2[0], pl);
-                const int t0 = __shfl_sync(0xffffffffu, i0, 31);
-                const int i1 = group_scan<32>(len2[1], pl);
-                sm.hoff[pl] = i0 - len2[0];
-                sm.hoff[pl + 32] = t0 + i1 - len2[1];
-                const int tot = t0 + __shfl_sync(0xffffffffu, i1, 31);
-                if (pl == 0) {
-                    sm.total = tot;
-                    sm.staged = tot <= CAP ? 1 : 0;
-                    if (sm.staged && tot > 0)
-                        mbar_expect(&sm.bar,
-                                    unsigned(tot) * unsigned(REC_N * sizeof(float4)) + unsigned(P.stage_extra));
-                }
+            for (int h = 0; h < 2; h++) {
+                const int c = 2 * pl + h;
+                const int cx = G.X0 - 2 + c / HY, cy = G.Y0 - 2 + c % HY;
+                const bool in = cx >= 0 && cx < nx && cy >= 0 && cy < ny;
+                len2[h] = in ? sm.cellstart[c][G.nzr - 1] - sm.cellstart[c][0] : 0;
+                sm.hstart[c] = sm.cellstart[c][0];
+                // bounds-checked build: a column whose range lies outside
+                // the record arrays is counted and not staged (len 0)
+                if (!range_ok(a.clk, sm.hstart[c], len2[h], P.n_init)) len2[h] = 0;
+                sm.hlen[c] = len2[h];
+            }
+            const int v = len2[0] + len2[1];
+            const int inc = group_scan<32>(v, pl);
+            sm.hoff[2 * pl] = inc - v;
+            sm.hoff[2 * pl + 1] = inc - v + len2[0];
+            const int tot = __shfl_sync(0xffffffffu, inc, 31);
+            if (pl == 0) {
+                sm.total = tot;
+                sm.staged = tot <= CAP ? 1 : 0;
+                if (ntg > 0 && sm.staged && tot > 0)
+                    mbar_expect(&sm.bar, unsigned(tot) * unsigned(REC_N * sizeof(float4)) + unsigned(P.stage_extra));
             }
         }
         pro_sync(PT);
@@ -845,7 +853,8 @@ __device__ __noinline__ void prepare_tile(const BatchTable &T, TileSmem<LPP, W> 
         if (ptid == 0) {
             sm.tile = t;
             sm.scene = s;
-            if (pend < sm.list_n) cp_async8(&sm.pre_entry, T.tile_list + pend);
+            const int k = atomicAdd(T.tile_next, 1);  // the next call's entry
+            if (k < sm.list_n) cp_async8(&sm.pre_entry, T.tile_list + k);
             else sm.pre_entry = make_int2(0, -1);
             sm.pre_ok = 1;
         }
