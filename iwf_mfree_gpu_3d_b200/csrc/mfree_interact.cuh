@@ -309,6 +309,27 @@ constexpr int NTC = TX * TY;           // target columns
 template <bool CSPM> __host__ __device__ constexpr int tile_threads() { return 640; }
 constexpr int TCAP = 320;              // targets per pass of a tile
 constexpr int QCAP_T = 96;             // in-support queue per target before the rescan path
+
+// The in-support queue and the column walk of a group.  A staged tile's
+// record indices are below the staging capacity, so its queue entries are 16
+// bits and a column-walk entry packs the column's end in the flattened order
+// (low 16 bits) with the record-minus-flattened index offset (high 16 bits,
+// signed): both lie within the capacity.  A tile read from global memory keeps
+// 32-bit entries, placed in the staging area that such a tile leaves idle.
+template <bool STAGED> struct Walk {
+    using Q = unsigned short;
+    using C = int;
+    static __device__ __forceinline__ C pack(int end, int off) { return int(unsigned(off) << 16) | end; }
+    static __device__ __forceinline__ int end(C w) { return w & 0xffff; }
+    static __device__ __forceinline__ int off(C w) { return w >> 16; }
+};
+template <> struct Walk<false> {
+    using Q = int;
+    using C = int2;
+    static __device__ __forceinline__ C pack(int end, int off) { return make_int2(end, off); }
+    static __device__ __forceinline__ int end(C w) { return w.x; }
+    static __device__ __forceinline__ int off(C w) { return w.y; }
+};
 constexpr int SMEM_LIMIT = 232448;     // per-block shared memory of sm_100
 constexpr long long WAIT_CYCLES = 1ll << 30;  // bound of a staging wait (~0.5 s of SM clock)
 
@@ -317,10 +338,10 @@ template <int LPP, int TILE_WARPS> struct TileSmem {
     float res[TCAP][NRES + 1];
     int tgt[TCAP];       // sorted index of each target of the pass
     int tcell[TCAP];     // its cell: target column << 16 | z
-    int q[TILE_WARPS][G][QCAP_T];
-    // per stencil column of a group's target: (end of its candidates in the
-    // flattened order, record index minus flattened index)
-    int2 cwalk[TILE_WARPS][G][25];
+    unsigned short q[TILE_WARPS][G][QCAP_T];
+    // per stencil column of a group's target: end of its candidates in the
+    // flattened order and record index minus flattened index (Walk<true>)
+    int cwalk[TILE_WARPS][G][25];
     int cellstart[NHC][CSROW];
     int hoff[NHC];       // staged offset of a halo column
     int hstart[NHC];     // global start of a halo column
@@ -385,7 +406,7 @@ template <int LPP> __device__ __forceinline__ int group_scan(int v, int sl) {
 // one target: stencil ranges, pass A (support, PSE, queue), CSPM pass over
 // the queue, pair pass over the queue, group reduction
 template <int LPP, bool CSPM, int COND, bool STAGED, class SM>
-__device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const float4 *RF, int rstride,
+__device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, float4 *spare, const float4 *RF, int rstride,
                                                int i, bool valid, int tt, int warp, int g, int sl, int lane, int X0,
                                                int Y0, int zl) {
     const Params &P = a.p;
@@ -420,8 +441,18 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
         I.h1 = 1.0f / I.h;
         I.fac = 0.31830988618379067f * I.h1 * I.h1 * I.h1;
     }
-    int2 *cw = sm.cwalk[warp][g];
-    int *qq = sm.q[warp][g];
+    using WK = Walk<STAGED>;
+    typename WK::C *cw;
+    typename WK::Q *qq;
+    if (STAGED) {
+        cw = reinterpret_cast<typename WK::C *>(sm.cwalk[warp][g]);
+        qq = reinterpret_cast<typename WK::Q *>(sm.q[warp][g]);
+    } else {  // 32-bit entries in the idle staging area
+        constexpr int NG = int(sizeof(sm.q) / sizeof(sm.q[0][0]));  // groups of the block
+        int *q32 = reinterpret_cast<int *>(spare);
+        qq = reinterpret_cast<typename WK::Q *>(q32 + (warp * SM::G + g) * QCAP_T);
+        cw = reinterpret_cast<typename WK::C *>(reinterpret_cast<int2 *>(q32 + NG * QCAP_T) + (warp * SM::G + g) * 25);
+    }
     int total;  // candidates of the target
     // ---- the 25 stencil columns as ranges of the record arrays, with their
     // prefix.  Without PSE (which sums every candidate of the 5x5x5 cells) the
@@ -482,7 +513,7 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
                 }
             }
             const int inc = group_scan<LPP>(l, sl);
-            if (c < 25) cw[c] = make_int2(carry + inc, b - (carry + inc - l));
+            if (c < 25) cw[c] = WK::pack(carry + inc, b - (carry + inc - l));
             carry += __shfl_sync(0xffffffffu, inc, (g * LPP) + LPP - 1);
         }
         total = carry;
@@ -496,8 +527,8 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
     for (int o = 16; o >= LPP; o >>= 1) maxtotal = max(maxtotal, __shfl_xor_sync(0xffffffffu, maxtotal, o));
     auto scan = [&](auto &&fn) {
         int col = 0;
-        int2 w = cw[0];
-        int cend = w.x, base = w.y;
+        typename WK::C w = cw[0];
+        int cend = WK::end(w), base = WK::off(w);
 #pragma unroll 2
         for (int k0 = 0; k0 < maxtotal; k0 += LPP) {
             const int k = k0 + sl;
@@ -506,8 +537,8 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
                 while (k >= cend) {  // k < total keeps col <= 24
                     col++;
                     w = cw[col];
-                    cend = w.x;
-                    base = w.y;
+                    cend = WK::end(w);
+                    base = WK::off(w);
                 }
             }
             int j = base + k;
@@ -524,8 +555,8 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
         // walks, then both loads, then the arithmetic, so the shared-memory
         // round trips overlap; the ballots keep the flattened order
         int col = 0;
-        int2 w = cw[0];
-        int cend = w.x, base = w.y;
+        typename WK::C w = cw[0];
+        int cend = WK::end(w), base = WK::off(w);
 #pragma unroll 1
         for (int k0 = 0; k0 < maxtotal; k0 += 2 * LPP) {
             const int ka = k0 + sl, kb = ka + LPP;
@@ -535,8 +566,8 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
                 while (ka >= cend) {
                     col++;
                     w = cw[col];
-                    cend = w.x;
-                    base = w.y;
+                    cend = WK::end(w);
+                    base = WK::off(w);
                 }
                 ja = base + ka;
                 if (!bounds_ok(a.clk, ja, rstride)) ja = 0;
@@ -545,8 +576,8 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, const 
                 while (kb >= cend) {
                     col++;
                     w = cw[col];
-                    cend = w.x;
-                    base = w.y;
+                    cend = WK::end(w);
+                    base = WK::off(w);
                 }
                 jb = base + kb;
                 if (!bounds_ok(a.clk, jb, rstride)) jb = 0;
@@ -993,13 +1024,13 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
                     const bool valid = tt < tn;
                     const int i = sm.tgt[valid ? tt : 0];
                     if (staged && COND == MFREE_COND_PSE && pse_zero)
-                        process_target<32, CSPM, MFREE_COND_NONE, true>(a, sm, sarr, CAP, i, valid, tt, warp, 0, lane, lane, X0,
+                        process_target<32, CSPM, MFREE_COND_NONE, true>(a, sm, sarr, sarr, CAP, i, valid, tt, warp, 0, lane, lane, X0,
                                                              Y0, zl);
                     else if (staged)
-                        process_target<32, CSPM, COND, true>(a, sm, sarr, CAP, i, valid, tt, warp, 0, lane, lane, X0,
+                        process_target<32, CSPM, COND, true>(a, sm, sarr, sarr, CAP, i, valid, tt, warp, 0, lane, lane, X0,
                                                              Y0, zl);
                     else
-                        process_target<32, CSPM, COND, false>(a, sm, gbase, gstride, i, valid, tt, warp, 0, lane, lane,
+                        process_target<32, CSPM, COND, false>(a, sm, sarr, gbase, gstride, i, valid, tt, warp, 0, lane, lane,
                                                               X0, Y0, zl);
                     done += TILE_WARPS;
                 } else if (LPP < 16 && rem <= 2 * TILE_WARPS) {
@@ -1008,13 +1039,13 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
                     const bool valid = tt < tn;
                     const int i = sm.tgt[valid ? tt : 0];
                     if (staged && COND == MFREE_COND_PSE && pse_zero)
-                        process_target<16, CSPM, MFREE_COND_NONE, true>(a, sm, sarr, CAP, i, valid, tt, warp, g2, sl2, lane, X0,
+                        process_target<16, CSPM, MFREE_COND_NONE, true>(a, sm, sarr, sarr, CAP, i, valid, tt, warp, g2, sl2, lane, X0,
                                                              Y0, zl);
                     else if (staged)
-                        process_target<16, CSPM, COND, true>(a, sm, sarr, CAP, i, valid, tt, warp, g2, sl2, lane, X0,
+                        process_target<16, CSPM, COND, true>(a, sm, sarr, sarr, CAP, i, valid, tt, warp, g2, sl2, lane, X0,
                                                              Y0, zl);
                     else
-                        process_target<16, CSPM, COND, false>(a, sm, gbase, gstride, i, valid, tt, warp, g2, sl2, lane,
+                        process_target<16, CSPM, COND, false>(a, sm, sarr, gbase, gstride, i, valid, tt, warp, g2, sl2, lane,
                                                               X0, Y0, zl);
                     done += 2 * TILE_WARPS;
                 } else {
@@ -1022,13 +1053,13 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
                     const bool valid = tt < tn;
                     const int i = sm.tgt[valid ? tt : 0];
                     if (staged && COND == MFREE_COND_PSE && pse_zero)
-                        process_target<LPP, CSPM, MFREE_COND_NONE, true>(a, sm, sarr, CAP, i, valid, tt, warp, g, sl, lane, X0,
+                        process_target<LPP, CSPM, MFREE_COND_NONE, true>(a, sm, sarr, sarr, CAP, i, valid, tt, warp, g, sl, lane, X0,
                                                               Y0, zl);
                     else if (staged)
-                        process_target<LPP, CSPM, COND, true>(a, sm, sarr, CAP, i, valid, tt, warp, g, sl, lane, X0,
+                        process_target<LPP, CSPM, COND, true>(a, sm, sarr, sarr, CAP, i, valid, tt, warp, g, sl, lane, X0,
                                                               Y0, zl);
                     else
-                        process_target<LPP, CSPM, COND, false>(a, sm, gbase, gstride, i, valid, tt, warp, g, sl, lane,
+                        process_target<LPP, CSPM, COND, false>(a, sm, sarr, gbase, gstride, i, valid, tt, warp, g, sl, lane,
                                                                X0, Y0, zl);
                     done += TILE_WARPS * G;
                 }
