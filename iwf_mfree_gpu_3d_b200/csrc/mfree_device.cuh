@@ -15,10 +15,11 @@
 //   The deviatoric stress is symmetric in the reference (every writer keeps
 //   S[c][r] == S[r][c]: predict/correct element-wise, Jaumann
 //   omega*S + S*omega^T, radial return), so 6 components are stored.
-//   half-step neighbour records, six float4 arrays (96 bytes per particle) in
-//   sorted order, written by the predictor and read by the pair loop; a halo
-//   column is one contiguous range of each array, staged into shared memory by
-//   one bulk copy per array:
+//   half-step neighbour records, six float4 (96 bytes) per particle in sorted
+//   order, written by the predictor and read by the pair loop: P alone, then
+//   V, A, B, R, C interleaved per particle (80 bytes); a halo column is one
+//   contiguous range of each of the two, staged into shared memory by two bulk
+//   copies:
 //     P = (x, y, z, tool_flag)      V = (vx, vy, vz, rho)
 //     A = sigma(xx, yy, zz, xy)     B = (sigma_xz, sigma_yz, c = sqrt(K/rho), h)
 //     R = R(xx, yy, zz, xy)         C = (R_xz, R_yz, T, m/rho)
@@ -151,8 +152,14 @@ struct Rec {
 };
 enum { REC_P = 0, REC_V, REC_A, REC_B, REC_R, REC_C, REC_N };
 
+// One allocation of REC_N * n_init float4: the P records at f[REC_P] = base
+// (stride 1), then the other five interleaved per particle, f[k] = base +
+// n_init + (k - 1) with stride REC_X; particle i's record k is
+// f[k][i * rec_stride(k)].
+constexpr int REC_X = REC_N - 1;
+__host__ __device__ constexpr int rec_stride(int k) { return k == REC_P ? 1 : REC_X; }
 struct Records {
-    float4 *f[REC_N];  // one allocation of REC_N * n_init float4, f[k] = base + k * n_init
+    float4 *f[REC_N];
 };
 
 struct Scratch {

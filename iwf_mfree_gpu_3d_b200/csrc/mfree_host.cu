@@ -385,9 +385,10 @@ int copy_records(mfree_ctx *c, std::vector<Rec> &dst) {
     CUDA_TRY(cudaMemcpyAsync(raw.data(), c->rec.f[0], sizeof(float4) * raw.size(), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     dst.resize(n);
-    for (int i = 0; i < n; i++)
-        dst[i] = Rec{raw[i], raw[size_t(n) + i], raw[2 * size_t(n) + i], raw[3 * size_t(n) + i],
-                     raw[4 * size_t(n) + i], raw[5 * size_t(n) + i]};
+    for (int i = 0; i < n; i++) {
+        const float4 *x = raw.data() + size_t(n) + size_t(i) * REC_X;  // V, A, B, R, C of particle i
+        dst[i] = Rec{raw[i], x[REC_V - 1], x[REC_A - 1], x[REC_B - 1], x[REC_R - 1], x[REC_C - 1]};
+    }
     return MFREE_OK;
 }
 
@@ -455,7 +456,8 @@ int alloc_ctx(int n, cudaStream_t stream, std::unique_ptr<mfree_ctx> &out) {
     {
         float4 *base = nullptr;
         if ((st = dalloc(c.get(), &base, size_t(REC_N) * n, L))) return bail(st);
-        for (int k = 0; k < REC_N; k++) c->rec.f[k] = base + size_t(k) * n;
+        c->rec.f[REC_P] = base;
+        for (int k = REC_V; k < REC_N; k++) c->rec.f[k] = base + size_t(n) + (k - REC_V);
     }
     if ((st = dalloc(c.get(), &c->scr.key, n, L))) return bail(st);
     if ((st = dalloc(c.get(), &c->scr.key_sorted, n, L))) return bail(st);

@@ -19,8 +19,9 @@
 // of the table from one work counter.  The tile's particles are 16 contiguous
 // ranges of the sorted order; the records their 5x5x5 stencils touch are the
 // 64 contiguous column ranges of the 8 x 8 x (D+4)-cell halo, staged into
-// shared memory with one bulk copy per column and record array (TMA
-// cp.async.bulk, completion counted on an mbarrier, bounded waits).  Each
+// shared memory with two bulk copies per column, its P records and the
+// interleaved rest (TMA cp.async.bulk, completion counted on an mbarrier,
+// bounded waits).  Each
 // target is served by a group of LPP lanes.  Pass A streams the target's
 // candidates (25 column ranges of the staged halo) through the lanes: support
 // test, PSE (which sums every stencil candidate) and a ballot that compacts
@@ -294,10 +295,11 @@ __device__ void epilogue(const StepArgs &a, int i, const float *res) {
 // ---------------------------------------------------------- pair kernel --
 // Tile = TX x TY x TZ cells of the cell grid; its particles are 16 contiguous
 // column ranges of the sorted order.  Their 5x5x5 stencils lie in the halo of
-// HX x HY x HZ cells: 64 contiguous column ranges of each record array, which
-// one bulk copy per column and array (cp.async.bulk, completion counted on an
-// mbarrier) stages into six shared-memory arrays.  A tile whose halo exceeds
-// the staging capacity reads the same records from global memory instead.
+// HX x HY x HZ cells: 64 contiguous column ranges of the P records and of the
+// interleaved rest, which two bulk copies per column (cp.async.bulk,
+// completion counted on an mbarrier) stage into shared memory in the same
+// layout.  A tile whose halo exceeds the staging capacity reads the same
+// records from global memory instead.
 constexpr int HX = TX + 4, HY = TY + 4;
 constexpr int CSROW = TILE_Z_MAX + 5;  // cell starts kept per halo column
 constexpr int NHC = HX * HY;           // halo columns
@@ -403,6 +405,13 @@ template <int LPP> __device__ __forceinline__ int group_scan(int v, int sl) {
     return v;
 }
 
+// the records of one kind at a fixed stride: P alone, the other five
+// interleaved per particle
+template <int S> struct RecView {
+    const float4 *__restrict__ p;
+    __device__ __forceinline__ const float4 &operator[](int j) const { return p[j * S]; }
+};
+
 // one target: stencil ranges, pass A (support, PSE, queue), CSPM pass over
 // the queue, pair pass over the queue, group reduction
 template <int LPP, bool CSPM, int COND, bool STAGED, class SM>
@@ -413,13 +422,12 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, float4
     const int nx = P.gnx, ny = P.gny, nz = P.gnz;
     const unsigned lt_mask = (1u << lane) - 1u;
     const unsigned gmask = LPP == 32 ? 0xffffffffu : (((1u << LPP) - 1u) << (g * LPP));
-    // the six record arrays at RF + k * rstride (shared memory or global)
-    const float4 *__restrict__ rP = RF + REC_P * rstride;
-    const float4 *__restrict__ rV = RF + REC_V * rstride;
-    const float4 *__restrict__ rA = RF + REC_A * rstride;
-    const float4 *__restrict__ rB = RF + REC_B * rstride;
-    const float4 *__restrict__ rR = RF + REC_R * rstride;
-    const float4 *__restrict__ rC = RF + REC_C * rstride;
+    // the records of rstride particles (shared memory or global): P at RF,
+    // V, A, B, R, C interleaved from RF + rstride
+    const float4 *X = RF + rstride;
+    const RecView<1> rP{RF};
+    const RecView<REC_X> rV{X + (REC_V - 1)}, rA{X + (REC_A - 1)}, rB{X + (REC_B - 1)}, rR{X + (REC_R - 1)},
+        rC{X + (REC_C - 1)};
     // the target's cell (from the pass's target table); its own records come
     // from the staged halo (its cell column is one of the halo's) or from
     // global memory
@@ -586,11 +594,11 @@ __device__ __forceinline__ void process_target(const StepArgs &a, SM &sm, float4
             float2 ta = make_float2(0.f, 0.f), tb = ta;
             if (acta) {
                 Pa = rP[ja];
-                if (COND == MFREE_COND_PSE) ta = reinterpret_cast<const float2 *>(rC + ja)[1];
+                if (COND == MFREE_COND_PSE) ta = reinterpret_cast<const float2 *>(&rC[ja])[1];
             }
             if (actb) {
                 Pb = rP[jb];
-                if (COND == MFREE_COND_PSE) tb = reinterpret_cast<const float2 *>(rC + jb)[1];
+                if (COND == MFREE_COND_PSE) tb = reinterpret_cast<const float2 *>(&rC[jb])[1];
             }
             bool insa = false, insb = false;
             if (acta) {
@@ -872,13 +880,17 @@ __device__ __noinline__ void prepare_tile(const BatchTable &T, TileSmem<LPP, W> 
         pro_sync(PT);
         if (sm.tpref[NTC] == 0) continue;  // an empty tile: take the next
         if (sm.staged && sm.total > 0) {
-            const float4 *gbase = a.r.f[0];  // the record arrays are one allocation: f[k] = f[0] + k * n_init
-            for (int q = ptid; q < REC_N * NHC; q += PT) {
+            // two copies a column: its P records to sarr, the interleaved rest
+            // to sarr + CAP (the record arrays are one allocation: P from
+            // f[REC_P], the rest from f[REC_P] + n_init)
+            const float4 *gbase = a.r.f[REC_P];
+            for (int q = ptid; q < 2 * NHC; q += PT) {
                 const int k = q / NHC, c = q - k * NHC;
                 const int len = sm.hlen[c];
-                if (len > 0)
-                    bulk_to_smem(sarr + k * CAP + sm.hoff[c], gbase + size_t(k) * P.n_init + sm.hstart[c],
-                                 unsigned(len) * unsigned(sizeof(float4)), &sm.bar);
+                const int w = k == 0 ? 1 : REC_X;
+                const size_t src = (k == 0 ? 0 : size_t(P.n_init)) + size_t(sm.hstart[c]) * w;
+                const int dst = (k == 0 ? 0 : CAP) + sm.hoff[c] * w;
+                if (len > 0) bulk_to_smem(sarr + dst, gbase + src, unsigned(len * w) * unsigned(sizeof(float4)), &sm.bar);
             }
         }
         if (ptid == 0) {
@@ -942,7 +954,7 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
         }
         const TileGeo geo = tile_geo(a.p, tile);
         const int X0 = geo.X0, Y0 = geo.Y0, zl = geo.zl;
-        const float4 *gbase = a.r.f[0];
+        const float4 *gbase = a.r.f[REC_P];  // tiles read from global memory: P, then the interleaved rest
         const int gstride = a.p.n_init;
         const int ntg = sm.tpref[NTC];
         const bool staged = sm.staged != 0;
@@ -985,11 +997,11 @@ __global__ void __launch_bounds__(tile_threads<CSPM>(), 1) kb_interact(BatchTabl
         // same results.  The test reads the staged halo after the wait.
         bool pse_zero = false;
         if (COND == MFREE_COND_PSE && staged && sm.total > 0 && !a.p.full_stencil) {
-            const float4 *rc = sarr + REC_C * CAP, *rp = sarr + REC_P * CAP;
+            const float4 *rc = sarr + CAP + (REC_C - 1), *rp = sarr;
             const float T0 = rc[0].z;
             bool u = true;
             for (int k = threadIdx.x; k < sm.total; k += TILE_THREADS) {
-                const float4 c = rc[k], p = rp[k];
+                const float4 c = rc[k * REC_X], p = rp[k];
                 u = u && c.z == T0 && isfinite(c.w) && isfinite(p.x) && isfinite(p.y) && isfinite(p.z);
             }
             pse_zero = __syncthreads_and(u) != 0;

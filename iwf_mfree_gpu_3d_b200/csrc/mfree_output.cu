@@ -198,9 +198,11 @@ int mfree_write_vtk(mfree_ctx *c, const char *path) {
     const int n = c->n_init;
     const State &S = c->st[c->cur];
     const float4 *src[SN_N] = {S.pos4, S.vel4, S.sa4, S.sb4, S.dsb4, S.fc4, S.ft4, c->rec.f[REC_V]};
-    for (int k = 0; k < SN_N; k++)
-        CUDA_TRY(cudaMemcpyAsync(J->d_snap + size_t(k) * n, src[k], sizeof(float4) * n, cudaMemcpyDeviceToDevice,
-                                 c->stream));
+    for (int k = 0; k < SN_N; k++) {  // (the V records are interleaved with four others: a pitched copy)
+        const size_t pitch = sizeof(float4) * (src[k] == c->rec.f[REC_V] ? rec_stride(REC_V) : 1);
+        CUDA_TRY(cudaMemcpy2DAsync(J->d_snap + size_t(k) * n, sizeof(float4), src[k], pitch, sizeof(float4), n,
+                                   cudaMemcpyDeviceToDevice, c->stream));
+    }
     CUDA_TRY(cudaEventRecord(J->snap, c->stream));
     CUDA_TRY(cudaStreamWaitEvent(J->stream, J->snap, 0));
     CUDA_TRY(cudaMemcpyAsync(J->h_snap, J->d_snap, sizeof(float4) * SN_N * size_t(n), cudaMemcpyDeviceToHost,

@@ -394,11 +394,12 @@ template <bool PREC> __device__ __forceinline__ void gather_predict_body(const S
     const float ir2 = 1.0f / (hs.rho * hs.rho);
     const Records &r = a.r;
     r.f[REC_P][i] = make_float4(hs.x, hs.y, hs.z, fc.w);  // raw tool_particle value
-    r.f[REC_V][i] = make_float4(hs.vx, hs.vy, hs.vz, hs.rho);
-    r.f[REC_A][i] = make_float4((hs.S[0] - prs) * ir2, (hs.S[1] - prs) * ir2, (hs.S[2] - prs) * ir2, hs.S[3] * ir2);
-    r.f[REC_B][i] = make_float4(hs.S[4] * ir2, hs.S[5] * ir2, sqrtf(P.K / hs.rho), pos.w);
-    r.f[REC_R][i] = make_float4(Rr[0], Rr[1], Rr[2], Rr[3]);
-    r.f[REC_C][i] = make_float4(Rr[4], Rr[5], hs.T, P.mass / hs.rho);
+    float4 *x = r.f[REC_V] + size_t(i) * REC_X;  // V, A, B, R, C interleaved
+    x[REC_V - 1] = make_float4(hs.vx, hs.vy, hs.vz, hs.rho);
+    x[REC_A - 1] = make_float4((hs.S[0] - prs) * ir2, (hs.S[1] - prs) * ir2, (hs.S[2] - prs) * ir2, hs.S[3] * ir2);
+    x[REC_B - 1] = make_float4(hs.S[4] * ir2, hs.S[5] * ir2, sqrtf(P.K / hs.rho), pos.w);
+    x[REC_R - 1] = make_float4(Rr[0], Rr[1], Rr[2], Rr[3]);
+    x[REC_C - 1] = make_float4(Rr[4], Rr[5], hs.T, P.mass / hs.rho);
     if (P.diagnostics) a.s.pos_half[i] = make_float4(hs.x, hs.y, hs.z, 0.f);
 }
 template <bool PREC> __global__ void __launch_bounds__(256) kb_gather_predict(BatchTable T) {
