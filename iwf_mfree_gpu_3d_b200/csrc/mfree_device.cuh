@@ -408,6 +408,27 @@ __device__ __forceinline__ float jc_yield_stress_screen(const Params &P, float e
     return a * b * c;
 }
 
+// A first screen without powf or logf, for the particles far below yield
+// (most of a cutting scene): with A > 0, B, C >= 0, eps_pl, eps_pl_dot >= 0
+// and 0 <= theta < 1 the yield stress is at least A (1 - theta^m) (the strain
+// and rate factors are at least 1), and theta^m is bounded from above by the
+// approximate exp2/log2 pair inflated by 1e-3.  A von Mises stress under 0.98
+// of that bound is under 0.99 of jc_yield_stress_screen as well (its FP32
+// rounding and the bound's error stay far inside the 1 % between 0.98 and
+// 0.99 while 1 - theta^m >= 1e-3), so the particle is elastic by the same
+// test as before and its results are the same bits.
+__device__ __forceinline__ bool jc_clearly_elastic(const Params &P, float svm, float eps_pl, float eps_pl_dot, float T) {
+    const float theta = (T - P.jc_Tref) / (P.jc_Tmelt - P.jc_Tref);
+    if (!(P.jc_A > 0.f && P.jc_B >= 0.f && P.jc_C >= 0.f && P.jc_m > 0.f && P.jc_epsdot_ref > 0.f && eps_pl >= 0.f &&
+          eps_pl_dot >= 0.f && theta >= 0.f && theta < 1.f))
+        return false;
+    float l2, p;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l2) : "f"(theta));  // theta = 0: -inf, and p = 0
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(p) : "f"(P.jc_m * l2));
+    const float c = 1.0f - 1.001f * p;
+    return c >= 1e-3f && svm < 0.98f * P.jc_A * c;
+}
+
 // Jaumann stress rate (actions_gpu.cu:134-190): S_t = 2G(epsdot - tr/3 I) + W S + S W^T,
 // L[a][b] = d v_a / d x_b, W(r,c) = (L_rc - L_cr)/2.  In/out order (xx, yy, zz, xy, xz, yz).
 __device__ __forceinline__ void jaumann(const float L[9], const float S[6], float G, float out[6]) {

@@ -226,7 +226,8 @@ __device__ void epilogue(const StepArgs &a, int i, const float *res) {
         float Tc = T;
         if (P.jc_clamp != 0.f) Tc = Tc > P.jc_Tmelt ? P.jc_Tmelt - 1.f : Tc;
         const float svm = 1.22474487139158905f * nS;
-        if (svm < 0.99f * jc_yield_stress_screen(P, eps, epsd, Tc) || svm < jc_yield_stress(P, eps, epsd, Tc)) {
+        if (jc_clearly_elastic(P, svm, eps, epsd, Tc) || svm < 0.99f * jc_yield_stress_screen(P, eps, epsd, Tc) ||
+            svm < jc_yield_stress(P, eps, epsd, Tc)) {
             epsd = 0.f;  // elastic
         } else {
             // FP64 secant from FP32 inputs, the result stored as float
