@@ -276,10 +276,26 @@ __device__ __forceinline__ void scatter_body(const StepArgs &a, int bid) {
     int blank = (i < P.n_init && key >= unsigned(P.num_cell)) ? 1 : 0;
     int total;
     int rank = block_exclusive_scan(blank, ws, total);
+    // one atomic per stretch of equal keys in the warp (the hash kernel's
+    // stretches): its first lane takes the stretch's length off the cell's
+    // count (which leaves count[] zero for the next step) and the stretch
+    // fills its slots in lane order, so it arrives in increasing index order
+    // and the per-cell fix-up below has little to move
+    const int lane = threadIdx.x & 31;
+    const unsigned counted = (i < P.n_init && !blank) ? key : 0xffffffffu;
+    const unsigned prev = __shfl_up_sync(0xffffffffu, counted, 1);
+    const bool start = lane == 0 || prev != counted;
+    const unsigned starts = __ballot_sync(0xffffffffu, start);
+    const unsigned upto = starts & ((2u << lane) - 1u);  // starts at or below this lane
+    const int head = 31 - __clz(upto);
+    const unsigned after = starts & ~((2u << lane) - 1u);
+    const int end = after ? __ffs(after) - 1 : 32;
+    int old = 0;
+    if (start && counted != 0xffffffffu) old = atomicSub(&a.s.count[counted], end - lane);
+    old = __shfl_sync(0xffffffffu, old, head);
     if (i >= P.n_init) return;
     if (!blank) {
-        int old = atomicSub(&a.s.count[key], 1);  // leaves count[] zero for the next step
-        const int d = a.s.first[key] + old - 1;
+        const int d = a.s.first[key] + old - (end - head) + (lane - head);
         if (bounds_ok(a.clk, d, P.n_init)) a.s.perm[d] = i;
     } else {
         const int d = N + a.s.blank_block[bid] + rank;
