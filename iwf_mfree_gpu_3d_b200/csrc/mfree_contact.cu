@@ -328,11 +328,8 @@ __device__ __forceinline__ void force_final_body(const StepArgs &a, int num_bloc
 }
 
 __global__ void __launch_bounds__(256) kb_finalize(BatchTable T) {
-    __shared__ StepArgs sa;
     const int s = find_scene(T.pblk, T.nscenes, blockIdx.x);
-    load_scene_args(sa, T, s);
-    __syncthreads();
-    finalize_body(sa, int(blockIdx.x) - T.pblk[s]);
+    finalize_body(scene_args(T, s), int(blockIdx.x) - T.pblk[s]);
 }
 // one block per scene
 __global__ void __launch_bounds__(256) kb_force_final(BatchTable T) {

@@ -122,6 +122,13 @@ __device__ __forceinline__ int find_scene(const int *__restrict__ prefix, int ns
     return lo;
 }
 
+// scene s's arguments for the parity of its current step, read in place
+// (read-only through the kernel, so the loads stay in L1 after the first warp)
+__device__ __forceinline__ const StepArgs &scene_args(const BatchTable &T, int s) {
+    const StepArgs *a0 = T.args + 2 * s;
+    return a0[a0->clk->parity & 1];
+}
+
 // copies scene s's arguments for the parity of its current step into shared
 // memory; every thread of the block calls it, a barrier must follow
 __device__ __forceinline__ void load_scene_args(StepArgs &dst, const BatchTable &T, int s) {

@@ -25,13 +25,11 @@ namespace mfree {
 
 // ----------------------------------------------------------------- clock --
 // batched kernels: block b of the launch is block b - prefix[s] of scene s,
-// whose arguments the block first copies into shared memory
+// whose arguments the block reads in place (a copy into shared memory, one
+// barrier per block, cost these short blocks more than it saved)
 template <class F> __device__ __forceinline__ void run_batched(const BatchTable &T, const int *prefix, F &&body) {
-    __shared__ StepArgs sa;
     const int s = find_scene(prefix, T.nscenes, blockIdx.x);
-    load_scene_args(sa, T, s);
-    __syncthreads();
-    body(sa, int(blockIdx.x) - prefix[s]);
+    body(scene_args(T, s), int(blockIdx.x) - prefix[s]);
 }
 
 // record_mode: 0 no, 1 yes, 2 every Params::record_every steps
