@@ -3,7 +3,8 @@ every index the kernels compute from data -- sort destinations, cell ranges,
 the pair kernel's cell starts, halo staging ranges, target and candidate
 records, the contact triangle ranges --
 is tested against its array and counted when outside, instead of being used.
-Small cases of every kernel variant run through it in a process of their own
+Small cases of every kernel variant (and a dense scene whose tiles read their
+records from global memory) run through it in a process of their own
 (the library is loaded once per process): no index may fall outside, and the
 physics must still match the FP64 oracle.  This stands in for a memory checker,
 which is not available on the GPU machines."""
@@ -54,6 +55,13 @@ b.step(10)
 b.sync()
 out["cases"]["batch"] = {"bounds_errors": sum(s.counters()["bounds_errors"] for s in sims)}
 b.close()
+# a dense scene (h = 2.2 dx): tiles read their records from global memory
+# and targets overflow their neighbour queue
+sim = api.Simulation.from_scene(scenes.orthogonal_cutting(30, 20, 16, hdx=2.2, cspm=True, conduction=2))
+for _ in range(3):
+    sim.step()
+out["cases"]["dense_global_records"] = {"bounds_errors": sim.counters()["bounds_errors"]}
+sim.close()
 print(json.dumps(out))
 """
 
