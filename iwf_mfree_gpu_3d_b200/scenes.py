@@ -411,6 +411,50 @@ def single_grain(nx: int = 400, ny: int = 160, nz: int = 64, dx: float = 1.0e-3,
     return sc
 
 
+def five_grain_scene(nx: int = 24, ny: int = 44, nz: int = 10, dx: float = 1.0e-3, v_tool: float = 3.0e-3,
+                     depth: float = 2.0, radius: float = 5.0, engage: float = 0.05, seed: int = 0,
+                     precision: int = 0) -> Scene:
+    """Five grains cutting one block, arranged as the reference's five-tool
+    single-grain setup arranges its grain copies (benchmarks_single_grain.cu:
+    29-471): a centre grain, two leading grains beside it at -+1.5 e in y, and
+    two trailing grains e behind the leading row at -+0.5 e in y, e = 2
+    radius (the grains do not overlap).  Each grain is the truncated icosphere
+    of single_grain (radius*dx, -10 deg rake) at depth*dx below the top
+    surface, all moving towards -x at v_tool: the leading row overlaps the
+    block's +x face by engage*dx and is in contact from the first step, the
+    trailing row reaches the block later.  Five tools in one contact pass, in
+    list order."""
+    sc = orthogonal_cutting(nx, ny, nz, dx=dx, v_tool=v_tool, depth=depth, seed=seed, precision=precision,
+                            name=f"five_grains_{nx}x{ny}x{nz}")
+    R = radius * dx
+    e = 2.0 * R
+    rake, cut = -10.0, 0.5
+    v, f = truncated_grain(R, rake_deg=rake, cut=cut)
+    lx = (nx - 1) * dx
+    tz = -depth * dx - v[:, 2].min()
+    a = math.radians(rake)
+    nxp, nzp = -math.cos(a), math.sin(a)
+    x_face = (cut * R - nzp * (-tz)) / nxp        # the face's x where it crosses the top surface
+    base = v.copy()
+    base[:, 0] += lx - engage * dx - x_face
+    base[:, 2] += tz
+    offsets = [(0.0, 0.0), (0.0, -1.5 * e), (0.0, 1.5 * e), (e, -0.5 * e), (e, 0.5 * e)]
+    algorithm = sc.tools[0].algorithm
+    sc.tools = []
+    for ox, oy in offsets:
+        g = base.copy()
+        g[:, 0] += ox
+        g[:, 1] += oy
+        sc.tools.append(Tool(verts=g.astype(np.float32), tris=f, vel=np.array([-v_tool, 0.0, 0.0], np.float32),
+                             algorithm=algorithm))
+    pad = 15.0 * dx
+    allv = np.concatenate([t.verts for t in sc.tools])
+    lo = (np.minimum(sc.pos[:, :3].min(0), allv.min(0)) - pad).astype(np.float32)
+    hi = (np.maximum(sc.pos[:, :3].max(0), allv.max(0)) + pad).astype(np.float32)
+    sc.grid_bbmin, sc.grid_bbmax, sc.blank_bbmin, sc.blank_bbmax = lo, hi, lo.copy(), hi.copy()
+    return sc
+
+
 # ---------------------------------------------------- mixed-size workloads --
 
 @dataclasses.dataclass

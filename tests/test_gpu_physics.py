@@ -113,6 +113,31 @@ def test_two_tools_against_fp64_oracle():
         e_series = np.linalg.norm(fg[:, k] - fo[:, k]) / np.linalg.norm(fo[:, k])
         print(f"tool {k}: force series rel L2 {e_series:.3e}")
         assert e_series < 1e-4, (k, e_series)  # measured 2.7e-5 and 4.5e-6
+
+
+def test_five_grains_against_fp64_oracle_and_the_reference_step():
+    """Five grains in the reference's five-tool arrangement (a centre grain,
+    two leading beside it, two trailing behind): the first step's contact
+    force of every tool against the FP64 oracle (the leading row in contact,
+    the trailing row not yet), then 40 steps checked as the single-grain
+    scenes are (against the reference's own GPU step where built)."""
+    sc = scenes.five_grain_scene()
+    sim, orc, fg, fo = _force_series(sc, 1)
+    for k in range(5):
+        ng, no = np.linalg.norm(fg[0, k]), np.linalg.norm(fo[0, k])
+        if k < 3:
+            assert no > 0, k  # the leading row touches the block from the first step
+            assert np.linalg.norm(fg[0, k] - fo[0, k]) < 1e-5 * no, (k, fg[0, k], fo[0, k])
+        else:
+            assert ng == 0 and no == 0, (k, ng, no)
+    for _ in range(39):
+        sim.step()
+        orc.step()
+    o = oracle_state(orc)
+    err = compare(gpu_state(sim), o, sc)
+    print("five grains, 40-step relative L2 vs FP64 oracle:", {k: f"{v:.2e}" for k, v in err.items()})
+    grain_checks(sc, sim, err, o, 40, "grain_40")
+    sim.close()
     sim.close()
 
 
