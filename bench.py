@@ -30,6 +30,7 @@ At N = 1 the line also carries the two systems forms, measured live:
     rate, duration, sizes and step counts are scaled down so the run takes
     seconds (the scaling is stated in the line).
   * "precision_form" (1M workload): the same step in the precision form;
+  * "small": the 8,000-particle configuration as stated, 1,000 steps;
   * "grain": the single-grain configuration (400 x 160 x 64 block plus the
     grain's tool particles, ~4.1M, compensated positions): particle-steps/s and
     HBM GB/s.
@@ -445,6 +446,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         line["grain"] = run_grain(args, opts)
     if world == 1 and not args.no_extras and args.workload == "1m":
         line["precision_form"] = run_precision_form(sc, args, opts)
+        line["small"] = run_small(args, opts)
     if world == 1 and not args.no_extras:
         line["batched"] = run_batched(args)
         line["serving"] = run_serve(args, tuple(line["batched"]["tiling"]))
@@ -503,6 +505,29 @@ def run_grain(args, opts) -> dict:
            "timing": "CUDA events around K graph replays, as the main line"}
     if not args.no_reference_gpu:
         out["reference_gpu"] = run_reference_gpu(sc, ms / steps, steps=5, warmup=2)
+    return out
+
+
+def run_small(args, opts) -> dict:
+    """The small configuration as stated: the 8,000-particle scene for 1,000
+    steps (graph replays), with the reference's own GPU step beside it (its
+    1,000-step parity is a test: tests/test_gpu_parity.py
+    test_1000_steps_small_configuration)."""
+    from iwf_mfree_gpu_3d_b200 import api
+    sc = make_scene("8k")
+    sim = api.Simulation.from_scene(sc, **opts)
+    sim.advance(max(args.warmup, 3), use_graph=True)
+    sim.sync()
+    steps = 1000
+    sim.timer_start()
+    sim.advance(steps, use_graph=True)
+    ms = sim.timer_stop()
+    sim.close()
+    value = sc.n * steps / (ms * 1e-3)
+    out = {"metric": "particle-steps/s", "value": value, "ms_per_step": ms / steps, "steps": steps,
+           "config": workload_config("8k", sc), "timing": "CUDA events around K graph replays, as the main line"}
+    if not args.no_reference_gpu:
+        out["reference_gpu"] = run_reference_gpu(sc, ms / steps, steps=100, warmup=3)
     return out
 
 

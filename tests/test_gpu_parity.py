@@ -11,7 +11,7 @@ import pytest
 import oracle
 from iwf_mfree_gpu_3d_b200 import api, scenes
 
-from helpers import grain_checks, check, compare, gpu_state, oracle_state
+from helpers import by_id, grain_checks, check, compare, gpu_state, oracle_state
 
 pytestmark = pytest.mark.gpu
 
@@ -174,6 +174,37 @@ def test_100_steps_against_fp64_oracle_8k():
     print("100-step relative L2 (FP32 CUDA vs FP64 oracle):", err)
     check(err, "8k_100")
     sim.close()
+
+
+def test_1000_steps_small_configuration():
+    """The small configuration as stated: 1000 steps of the 8,000-particle
+    scene against the FP64 oracle.  Over that many steps of contact the FP32
+    trajectories part from FP64 as far as the reference's own GPU step does,
+    so where that build is at hand the CUDA path's error may be at most a
+    quarter above the reference's (field by field); elsewhere the bounds of
+    8k_1000."""
+    sc = scenes.small_scene()
+    sim = _sim(sc)
+    orc = oracle.Oracle(sc, prec=64)
+    for _ in range(1000):
+        sim.step()
+        orc.step()
+    o = oracle_state(orc)
+    err = compare(gpu_state(sim), o, sc)
+    sim.close()
+    print("1000-step relative L2 (FP32 CUDA vs FP64 oracle):", {k: f"{v:.2e}" for k, v in err.items()})
+    assert err["blank_mismatch"] == 0
+    from baseline import refgpu
+    if not refgpu.available(refgpu.variant_of(sc)):
+        check(err, "8k_1000")
+        return
+    names = ["POS", "VEL", "S", "EPS_PL", "T", "RHO"]
+    st = refgpu.run(sc, 0, 1000, state=True)["state"]
+    r = {n: by_id(st["ID"], st[n].astype(np.float64)) for n in names + ["BLANKED"]}
+    e_ref = compare(r, o, sc, names)
+    print("reference GPU step vs FP64 oracle:", {k: f"{v:.2e}" for k, v in e_ref.items()})
+    for f in names:
+        assert err[f] <= 1.25 * e_ref[f] + 1e-7, (f, err[f], e_ref[f])
 
 
 def test_graph_replay_equals_eager_steps():
